@@ -1,0 +1,447 @@
+#!/usr/bin/env python
+"""Benchmark of the B200 lighting hot path (ReSTIR + SDF visibility + SVGF).
+
+A step is one frame of the hot path (the 8 lighting entry points of
+lighting.wgsl and the 3 SVGF stages) over the 1920x1200 room of 24 meshes
+(128^3 f32 SDF grids, 8 emitters, 1024 VPL paths, 3 bounces, orbit 1 deg and
+dolly 0.05 m per frame).  Prints one JSON line.
+
+  python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference]
+
+ours      : inputs (per-frame G-buffers, VPL pools) resident in HBM before the
+            timed region; `value` is device-timed Mpix-frames/s, `e2e` the same
+            through the C-ABI with host-pinned inputs copied in and the filtered
+            image copied out every step.
+reference : the CPU restatement of the reference's WGSL (oracle/, FP32, all
+            host threads) on the same workload; rank 0 only.
+N > 1 runs independent replicas (one session per GPU, no collective on the
+path); value is the sum of pixels over the max device time of the ranks.
+"""
+from __future__ import annotations
+
+import argparse
+import datetime
+import json
+import os
+import statistics
+import subprocess
+import sys
+import threading
+import time
+
+import numpy as np
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, ROOT)
+
+# Algorithmic bytes per pixel and kernel for the f32 G-buffer / f32 radiance
+# schedule (every surface counted once per kernel that touches it; neighbour
+# taps are cache traffic, not HBM):
+#   reuse  = G-buffer 44 (depth 4, normal 12, colour 12, params 8, motion 8)
+#            + previous depth/normal 16 + history reservoirs D/I 64
+#            + reservoirs [1] D/I written 64                          = 188
+#   shade  = G-buffer 36 (no motion) + reservoirs [1] 64 + [2] written 64
+#            + direct f32x4 16 + noisy f32x4 16                       = 196
+#   svgf_temporal = noisy 16 + G-buffer 44 + feedback 16 + moments 16
+#            + previous depth/normal 16 + temporal 16 + moments 16    = 140
+#   svgf_variance = temporal 16 + moments 16 + G-buffer guides 36
+#            + output 16                                              =  84
+#   atrous = input 16 + guides 36 + output 16                         =  68 (x4)
+#   history copy = depth+normal read 20 + write 20                    =  40
+ALG_BYTES = {"reuse": 188, "shade": 196, "svgf_temporal": 140, "svgf_variance": 84, "atrous": 4 * 68,
+             "history": 40}
+STAGES = ["archive", "reuse", "shade", "svgf_temporal", "svgf_variance", "atrous", "history"]
+KERNELS_PER_FRAME_FUSED = 2 + 2 + 4  # reuse, shade, svgf temporal, variance, 4 a-trous
+
+
+def parse():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=24)
+    ap.add_argument("--warmup", type=int, default=8)
+    ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
+    ap.add_argument("--config", type=int, default=1)
+    ap.add_argument("--width", type=int, default=0)
+    ap.add_argument("--height", type=int, default=0)
+    ap.add_argument("--plain", action="store_true", help="one kernel per reference entry point")
+    ap.add_argument("--no-e2e", action="store_true")
+    ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--cpu-seconds", type=float, default=15.0, help="CPU work budget of the cpu_baseline sample")
+    ap.add_argument("--reference-seconds", type=float, default=150.0, help="CPU budget of the reference arm")
+    return ap.parse_args()
+
+
+def rank_info():
+    return int(os.environ.get("RANK", 0)), int(os.environ.get("WORLD_SIZE", 1)), int(os.environ.get("LOCAL_RANK", 0))
+
+
+def workload_spec(args):
+    from instantradiositytest_b200.workload import preset_spec
+
+    over = {}
+    if args.width:
+        over["width"] = args.width
+    if args.height:
+        over["height"] = args.height
+    return preset_spec(args.config, **over)
+
+
+def describe(spec, frames, schedule):
+    return {
+        "workload": f"room of {6 if not spec.room_single_mesh else 1}+{spec.n_boxes}+{spec.n_spheres} meshes, "
+                    f"{spec.width}x{spec.height}, {frames} frames",
+        "width": spec.width, "height": spec.height, "frames": frames,
+        "meshes": (1 if spec.room_single_mesh else 6) + spec.n_boxes + spec.n_spheres,
+        "sdf": f"{spec.sdf_resolution}^3 {'f16' if spec.sdf_format else 'f32'}",
+        "emitters": spec.n_lights, "vpl_paths": spec.vpl_count, "bounces": spec.vpl_bounces,
+        "restir": "8+8 candidates, 4 neighbours r=12, 4-frame history", "sdf_march": "96 steps, eps 0.001, k=16",
+        "svgf": "32-frame history, 4 a-trous", "storage": "f32 G-buffer, f32 radiance, f32 moments",
+        "schedule": schedule,
+        "l2": "inputs larger than L2: a distinct 120 MB G-buffer per frame, ~1 GB working set per frame",
+        "parallelism": "replicas",
+    }
+
+
+class Clocks:
+    """nvidia-smi samples (SM clock, reasons) during the timed region."""
+
+    Q = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+         "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+         "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, index):
+        self.index = index
+        self.proc = None
+        self.lines = []
+
+    def start(self):
+        try:
+            self.proc = subprocess.Popen(["nvidia-smi", f"--id={self.index}", f"--query-gpu={self.Q}",
+                                          "--format=csv,noheader,nounits", "-lms", "200"],
+                                         stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True)
+            self.t = threading.Thread(target=self._read, daemon=True)
+            self.t.start()
+        except OSError:
+            self.proc = None
+
+    def _read(self):
+        for line in self.proc.stdout:
+            self.lines.append(line.strip())
+
+    def stop(self):
+        if not self.proc:
+            return None
+        self.proc.terminate()
+        try:
+            self.proc.wait(timeout=5)
+        except subprocess.TimeoutExpired:
+            self.proc.kill()
+        sm, mx, reasons = [], 0.0, set()
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        for ln in self.lines:
+            parts = [p.strip() for p in ln.split(",")]
+            if len(parts) < 9:
+                continue
+            try:
+                sm.append(float(parts[1]))
+                mx = max(mx, float(parts[2]))
+            except ValueError:
+                continue
+            for n, v in zip(names, parts[5:9]):
+                if v.lower().startswith("active"):
+                    reasons.add(n)
+        if not sm:
+            return None
+        return {"sm_mhz": statistics.median(sm), "sm_max_mhz": mx, "reasons": sorted(reasons), "samples": len(sm)}
+
+
+def measured_peak():
+    try:
+        with open(os.path.join(ROOT, "MEASURED_PEAKS.json")) as fh:
+            return float(json.load(fh)["hbm_gbs"]), "measured"
+    except (OSError, KeyError, ValueError):
+        return 6650.0, "fallback"
+
+
+def ncu_traffic():
+    """dram bytes per launch of the shade kernel from the committed ncu
+    summary (profiles/shade_kernel_1920x1200.md, line `dram_bytes_per_launch:`)."""
+    path = os.path.join(ROOT, "profiles", "shade_kernel_1920x1200.md")
+    try:
+        for line in open(path):
+            if line.startswith("dram_bytes_per_launch:"):
+                return float(line.split(":", 1)[1].strip())
+    except OSError:
+        pass
+    return None
+
+
+# ------------------------------------------------------------------ CPU legs
+def cpu_run(spec, steps, warmup, budget_s, threads=0):
+    """Time the oracle (FP32 restatement of the WGSL) on a band of rows of the
+    workload: frames 0..warmup-1 untimed, then `steps` timed frames.  The band
+    height is chosen from a probe so the whole run stays near budget_s."""
+    from instantradiositytest_b200.workload import Workload
+    from oracle import Oracle, OracleScene
+
+    wl = Workload(spec)
+    W, H = wl.width, wl.height
+    orc = Oracle(W, H, wl.settings.vpl_count, wl.settings.restir_max_history, 0, False, threads)
+    prev = None
+    cache = {}
+
+    def inputs(i):
+        if i not in cache:
+            f, obj, nodes, lights = wl.frame(i)
+            cache.clear()
+            cache[i] = (f, obj, nodes, lights, wl.gbuffer_cpu(f), wl.vpls_cpu(f, obj, lights))
+        return cache[i]
+
+    def run(i, rows):
+        nonlocal prev
+        f, obj, nodes, lights, g, v = inputs(i)
+        p = prev if prev is not None else np.zeros_like(v)
+        y0 = (H - rows) // 2
+        orc.set_rows(y0, y0 + rows)
+        t = time.perf_counter()
+        orc.frame(f, OracleScene(obj, wl.meshes, nodes, lights, wl.atlas), g, v, p,
+                  wl.settings.svgf_iterations)
+        dt = time.perf_counter() - t
+        prev = v
+        return dt
+
+    probe_rows = min(H, 16)
+    t_probe = run(0, probe_rows)
+    per_row = max(t_probe / probe_rows, 1e-6)
+    rows = int(max(8, min(H, budget_s / max(steps + warmup, 1) / per_row)))
+    for i in range(1, warmup + 1):
+        run(i, rows)
+    total = 0.0
+    for i in range(warmup + 1, warmup + 1 + steps):
+        total += run(i, rows)
+    threads_used = orc.threads
+    orc.close()
+    wl.close()
+    px = rows * W * steps
+    return {"value": px / total / 1e6, "seconds": total, "rows": rows, "steps": steps, "threads": threads_used,
+            "sample": f"{rows} of {H} rows (centre band) x {W} columns, {steps} timed frames after "
+                      f"{warmup + 1} warm-up frames, full SVGF + lighting on the band"}
+
+
+def reference_arm(args):
+    rank, world, _ = rank_info()
+    if rank != 0:
+        return
+    spec = workload_spec(args)
+    r = cpu_run(spec, args.steps, args.warmup, args.reference_seconds)
+    frames = args.steps + args.warmup
+    line = {
+        "metric": "Mpix-frames/s", "value": r["value"], "unit": "Mpix-frames/s", "n_gpus": args.gpus,
+        "steps": args.steps, "warmup": args.warmup, "ms_per_step": 1000.0 * r["seconds"] / r["steps"],
+        "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f32", "data": "synthetic",
+        "impl": "reference",
+        "config": describe(spec, frames, "CPU restatement of the WGSL passes (oracle/), OpenMP over pixels"),
+        "cpu_baseline": {"value": r["value"], "unit": "Mpix-frames/s", "cores": r["threads"], "kind": "port",
+                         "sample": r["sample"]},
+        "e2e": {"value": r["value"], "unit": "Mpix-frames/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
+        "note": "the reference's WGSL cannot run here (no Rust toolchain, no Vulkan/graphics stack); "
+                "this arm is its CPU restatement",
+    }
+    print(json.dumps(line), flush=True)
+
+
+# ------------------------------------------------------------------ our arm
+def ours(args):
+    import ctypes as C
+
+    import torch
+
+    from instantradiositytest_b200 import _lib as L
+    from instantradiositytest_b200.runtime import (Context, Scene, Session, gbuffer_device_alloc, session_desc,
+                                                   stream_handle)
+    from instantradiositytest_b200.workload import Workload, alloc_gbuffer
+
+    rank, world, local = rank_info()
+    dist = None
+    if world > 1:
+        import torch.distributed as dist
+
+        torch.cuda.set_device(local)
+        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=180))
+    else:
+        torch.cuda.set_device(0)
+    dev = torch.cuda.current_device()
+    spec = workload_spec(args)
+    wl = Workload(spec)
+    W, H, P = wl.width, wl.height, wl.width * wl.height
+    K, Wm = args.steps, args.warmup
+    n_frames = K + Wm
+    ctx = Context(dev)
+    scene = Scene(ctx, wl.meshes, wl.atlas, wl.sdf_format)
+    fused = not args.plain
+    sess = Session(ctx, session_desc(wl.settings, L.GBUFFER_F32, L.RADIANCE_F32, fused, False))
+    stream = torch.cuda.current_stream()
+    sh = stream_handle()
+
+    # ---- inputs resident in HBM: per-frame G-buffers (CUDA producer) and VPLs
+    frames, gbufs, vpls = [], [], []
+    for i in range(n_frames):
+        f, obj, nodes, lights = wl.frame(i)
+        t, gs = gbuffer_device_alloc(H, W, L.GBUFFER_F32)
+        L.check(L.lib.irt_gbuffer_render(ctx.handle, wl.handle, C.byref(f), None, L.GBUFFER_F32, gs.depth,
+                                         gs.normal, gs.color, gs.params, gs.motion, sh), ctx.handle, "gbuffer")
+        v = wl.vpls_cpu(f, obj, lights)
+        frames.append((f, obj, nodes, lights))
+        gbufs.append((t, gs))
+        vpls.append(torch.from_numpy(v.view(np.uint8)).cuda())
+    torch.cuda.synchronize()
+    zero_vpls = torch.zeros_like(vpls[0])
+
+    def render(i):
+        f, obj, nodes, lights = frames[i]
+        scene.update(obj, nodes, lights, sh)
+        prev = vpls[i - 1] if i > 0 else zero_vpls
+        sess.render(scene, f, gbufs[i][1], C.c_void_p(vpls[i].data_ptr()), C.c_void_p(prev.data_ptr()), sh)
+
+    for i in range(Wm):
+        render(i)
+    torch.cuda.synchronize()
+    if dist:
+        dist.barrier()
+    sess.set_profiling(True)
+    clocks = Clocks(dev)
+    clocks.start()
+    torch.cuda.synchronize()
+    if dist:
+        dist.barrier()
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    e0.record(stream)
+    for i in range(Wm, Wm + K):
+        render(i)
+    e1.record(stream)
+    torch.cuda.synchronize()
+    if dist:
+        dist.barrier()
+    clk = clocks.stop()
+    ms = e0.elapsed_time(e1)
+    stage = np.array([sess.pass_ms(i) for i in range(Wm, Wm + K)])  # [K, 8]
+    sess.set_profiling(False)
+    assert sess.check() == L.IRT_OK, ctx.error()
+    ms_max = ms
+    if dist:
+        tt = torch.tensor([ms], device="cuda")
+        dist.all_reduce(tt, op=dist.ReduceOp.MAX)
+        ms_max = float(tt.item())
+    value = world * P * K / (ms_max / 1000.0) / 1e6
+    frame_ms = stage[:, 7]
+
+    # ---- roofline of the dominant kernel
+    names = STAGES
+    mean_ms = stage[:, :7].mean(0)
+    kernel_idx = {n: i for i, n in enumerate(names)}
+    candidates = ["reuse", "shade", "svgf_temporal", "svgf_variance", "atrous"]
+    dominant = max(candidates, key=lambda n: mean_ms[kernel_idx[n]])
+    peak, peak_kind = measured_peak()
+
+    def ach(n):
+        return ALG_BYTES[n] * P / (mean_ms[kernel_idx[n]] / 1000.0) / 1e9
+
+    achieved = ach(dominant)
+    traffic = ncu_traffic() if dominant == "shade" else None
+    roofline = {"bound": "hbm", "kernel": dominant, "achieved": achieved, "peak": peak, "unit": "GB/s",
+                "frac": achieved / peak, "traffic": traffic, "peak_source": peak_kind,
+                "alg_bytes_per_pixel": ALG_BYTES[dominant],
+                "kernels": {n: {"ms": float(mean_ms[kernel_idx[n]]), "alg_GBps": ach(n), "frac": ach(n) / peak}
+                            for n in candidates},
+                "note": "shade = spatial reuse + resolve with the SDF soft-shadow march; its time is the "
+                        "march (FP32/latency bound), so its HBM fraction is low by construction"}
+
+    # ---- e2e through the C-ABI with host buffers
+    e2e = None
+    if not args.no_e2e:
+        ring = min(8, n_frames)
+        host = []
+        for i in range(ring):
+            f, obj, nodes, lights = frames[Wm + i] if Wm + i < n_frames else frames[i]
+            g = {k: torch.from_numpy(v.view(np.uint8) if v.dtype != np.uint8 else v).pin_memory()
+                 for k, v in wl.gbuffer_cpu(f, L.GBUFFER_F32).items()}
+            v = torch.from_numpy(wl.vpls_cpu(f, obj, lights).view(np.uint8)).pin_memory()
+            host.append((f, obj, nodes, lights, g, v))
+        dev_g, dev_gs = gbuffer_device_alloc(H, W, L.GBUFFER_F32)
+        dv = [torch.empty_like(vpls[0]), torch.empty_like(vpls[0])]
+        out_ptr, out_bytes = sess.buffer_ptr(L.BUF_FILTERED)
+        out_dev = sess.buffer(L.BUF_FILTERED, torch.uint8)
+        out_host = torch.empty(out_bytes, dtype=torch.uint8).pin_memory()
+        h2d = sum(int(t.numel()) for t in host[0][4].values()) + int(host[0][5].numel())
+        d2h = int(out_bytes)
+        K2 = min(K, 16)
+
+        def e2e_step(j, idx):
+            f, obj, nodes, lights, g, v = host[j % ring]
+            for k in ("depth", "normal", "color", "params", "motion"):
+                dev_g[k].copy_(g[k].view(-1), non_blocking=True)
+            cur, prv = dv[idx % 2], dv[(idx + 1) % 2]
+            cur.copy_(v, non_blocking=True)
+            scene.update(obj, nodes, lights, sh)
+            sess.render(scene, f, dev_gs, C.c_void_p(cur.data_ptr()), C.c_void_p(prv.data_ptr()), sh)
+            out_host.copy_(out_dev, non_blocking=True)
+
+        for j in range(3):
+            e2e_step(j, j)
+        torch.cuda.synchronize()
+        if dist:
+            dist.barrier()
+        a0, a1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        a0.record(stream)
+        for j in range(K2):
+            e2e_step(j, j + 3)
+        a1.record(stream)
+        torch.cuda.synchronize()
+        ems = a0.elapsed_time(a1)
+        if dist:
+            tt = torch.tensor([ems], device="cuda")
+            dist.all_reduce(tt, op=dist.ReduceOp.MAX)
+            ems = float(tt.item())
+        e2e = {"value": world * P * K2 / (ems / 1000.0) / 1e6, "unit": "Mpix-frames/s", "h2d_bytes_per_step": h2d,
+               "d2h_bytes_per_step": d2h, "steps": K2, "ms_per_step": ems / K2,
+               "path": "irt_scene_update + irt_render_frame (C-ABI) with pinned host G-buffer and VPL pool "
+                       "copied in and the filtered image copied out every step"}
+
+    # ---- CPU baseline (rank 0, N = 1)
+    cpu = None
+    if rank == 0 and world == 1 and not args.no_cpu_baseline:
+        r = cpu_run(spec, 1, 1, args.cpu_seconds)
+        cpu = {"value": r["value"], "unit": "Mpix-frames/s", "cores": r["threads"], "kind": "port",
+               "sample": r["sample"]}
+
+    if rank == 0:
+        line = {
+            "metric": "Mpix-frames/s", "value": value, "unit": "Mpix-frames/s", "n_gpus": world, "steps": K,
+            "warmup": Wm, "ms_per_step": ms_max / K, "higher_is_better": True, "scaling": "weak",
+            "vs_baseline": None, "dtype": "f32", "data": "synthetic",
+            "config": describe(spec, n_frames, "fused" if fused else "plain"),
+            "p50_frame_ms": float(np.percentile(frame_ms, 50)), "p99_frame_ms": float(np.percentile(frame_ms, 99)),
+            "stage_ms": {n: float(mean_ms[i]) for i, n in enumerate(names)},
+            "roofline": roofline, "cpu_baseline": cpu, "e2e": e2e,
+            "gpu_launches": K * (KERNELS_PER_FRAME_FUSED if fused else 14),
+            "clocks": clk,
+        }
+        print(json.dumps(line), flush=True)
+    sess.close()
+    scene.close()
+    ctx.close()
+    if dist:
+        dist.barrier()
+        dist.destroy_process_group()
+
+
+def main():
+    args = parse()
+    if args.impl == "reference":
+        reference_arm(args)
+    else:
+        ours(args)
+
+
+if __name__ == "__main__":
+    main()

@@ -1,0 +1,358 @@
+/*
+ * irt.h — C-ABI of the B200 lighting hot path (ReSTIR direct + VPL indirect,
+ * SDF soft-shadow visibility, SVGF) of the instantradiositytest renderer.
+ *
+ * The boundary replaces the wgpu binding contract of the reference's compute
+ * passes:
+ *   group 0 (scene)    common.wgsl:17-30,  src/renderer.rs:1185-1204
+ *   group 1 (G-buffer) lighting.wgsl:1-5,  src/renderer.rs:1314-1324
+ *   group 2 (per pass) lighting.wgsl:6-21, src/renderer.rs:1617-1674,
+ *                      svgf.wgsl:8-17,     src/svgf.rs:163-211
+ * and the pass schedule of Renderer::encode (src/renderer.rs:1873-1928) and
+ * Svgf::encode (src/svgf.rs:140-261).
+ *
+ * Conventions: every call returns irt_status (0 = ok, negative = error) and
+ * never throws; irt_last_error() gives the message of the last failure on a
+ * context.  Device pointers are plain CUDA device addresses; `stream` is a
+ * cudaStream_t passed as void* (NULL = legacy default stream).  No torch
+ * types appear here.
+ */
+#ifndef IRT_H
+#define IRT_H
+
+#include <stddef.h>
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+typedef int32_t irt_status;
+#define IRT_OK 0
+#define IRT_E_INVALID (-1)     /* bad argument / failed validation          */
+#define IRT_E_CUDA (-2)        /* a CUDA runtime call failed                 */
+#define IRT_E_ADMISSION (-3)   /* session would exceed the HBM budget        */
+#define IRT_E_NOMEM (-4)       /* host allocation failed                     */
+#define IRT_E_STATE (-5)       /* call made in the wrong order               */
+#define IRT_E_DEVICE (-6)      /* a kernel reported a bounded-loop violation */
+#define IRT_E_NODEVICE (-7)    /* no CUDA device is visible                  */
+
+/* ---------------------------------------------------------------------------
+ * Byte layouts shared with the caller.  Sizes are the reference's GPU struct
+ * sizes (src/renderer.rs:2253-2261, common.wgsl:3-16); matrices are
+ * column-major 4x4 f32 like glam::Mat4 and WGSL mat4x4<f32>.
+ * ------------------------------------------------------------------------- */
+typedef struct irt_mat4 { float m[16]; } irt_mat4;
+
+/* common.wgsl:3-8, src/renderer.rs:52-66 — 384 bytes. */
+typedef struct irt_frame {
+    irt_mat4 vp, inv_vp, previous_vp, previous_inv_vp;
+    float camera[4];
+    uint32_t size[4];     /* width, height, frame_index, generation          */
+    uint32_t counts[4];   /* lights, vpl_count, vpl_bounces, objects         */
+    uint32_t restir[4];   /* direct cands, vpl cands, spatial nbrs, radius   */
+    float temporal[4];    /* history weight, depth thr, normal thr, max hist */
+    float sdf[4];         /* max steps, hit epsilon, soft-shadow k, 0        */
+    float rr[4];          /* rr min, rr max, restir max history, 0           */
+    uint32_t flags[4];    /* history enabled, previous generation, debug, 0  */
+} irt_frame;
+
+/* common.wgsl:9, src/renderer.rs:8-15 — 208 bytes.
+ * info = [mesh id, material id, bits(uniform scale), bits(voxel diag*scale)] */
+typedef struct irt_object {
+    irt_mat4 model, previous, inverse;
+    uint32_t info[4];
+} irt_object;
+
+/* common.wgsl:10, src/renderer.rs:16-28 — 128 bytes.
+ * field = [atlas origin x,y,z, resolution]; grid = [1/spacing xyz, |spacing|];
+ * geometry_lo.w = certified box flag; geometry_hi.w = 1/Lipschitz bound. */
+typedef struct irt_mesh {
+    float lo[4], hi[4];
+    uint32_t geometry[4];
+    uint32_t field[4];
+    float grid[4];
+    float geometry_lo[4], geometry_hi[4];
+    float enclosing_sphere[4];
+} irt_mesh;
+
+/* common.wgsl:11, src/renderer.rs:29-36 — 64 bytes. */
+typedef struct irt_material {
+    float color[4], params[4];
+    int32_t textures[4];
+    uint32_t channels[4];
+} irt_material;
+
+/* common.wgsl:12, src/renderer.rs:37-43 — 48 bytes.
+ * color_type.w > 0.5 marks a spot light. */
+typedef struct irt_light {
+    float position_strength[4], direction_angle[4], color_type[4];
+} irt_light;
+
+/* common.wgsl:13, src/scene.rs:136-143 — 64 bytes. */
+typedef struct irt_vertex {
+    float position[4], normal[4], tangent[4], uv[4];
+} irt_vertex;
+
+/* common.wgsl:14, src/renderer.rs:44-50 — 48 bytes.
+ * info = [left|object, right, leaf flag, escape index] (preorder). */
+typedef struct irt_node {
+    float lo[4], hi[4];
+    uint32_t info[4];
+} irt_node;
+
+/* common.wgsl:15 — 48 bytes. */
+typedef struct irt_vpl {
+    float position[4], normal[4], flux[4];
+} irt_vpl;
+
+/* common.wgsl:16 — 32 bytes; the device stores reservoirs in exactly this
+ * layout (one 32-byte sector per pixel, read as two 128-bit vectors). */
+typedef struct irt_reservoir {
+    uint32_t id, source, count, age;
+    float sum, selected_target, pdf;
+    uint32_t generation;
+} irt_reservoir;
+
+/* settings.json / src/settings.rs:5-28. */
+typedef struct irt_settings {
+    uint32_t render_width, render_height;
+    uint32_t vpl_count, vpl_max_bounces;
+    float vpl_rr_min_survival, vpl_rr_max_survival;
+    uint32_t restir_direct_candidates, restir_vpl_candidates;
+    uint32_t restir_spatial_neighbors, restir_spatial_radius;
+    uint32_t restir_max_history, svgf_iterations;
+    float depth_threshold, normal_threshold, temporal_history_weight;
+    uint32_t temporal_max_history;
+    uint32_t sdf_max_steps;
+    float sdf_hit_epsilon, sdf_soft_shadow_k, target_frame_ms;
+} irt_settings;
+
+/* Reference defaults (settings.json:1-22) with serde defaults for
+ * restir_max_history / svgf_iterations (src/settings.rs:29-34). */
+void irt_settings_default(irt_settings* out);
+/* Same checks and messages as Settings::validate (src/settings.rs:42-105).
+ * Writes the failing rule into msg (may be NULL). */
+irt_status irt_settings_validate(const irt_settings* s, char* msg, size_t msg_len);
+
+/* ---------------------------------------------------------------------------
+ * Storage formats.
+ * ------------------------------------------------------------------------- */
+/* G-buffer planes (the reference's group-1 textures), all W*H row-major:
+ *   F32:    depth f32, normal f32x4, color f32x4, params f32x2, motion f32x2
+ *   F16:    depth f32, normal f16x4, color f16x4, params f16x2, motion f16x2
+ *           (= the reference's Depth32Float / Rgba16Float / Rg16Float targets,
+ *            src/renderer.rs:1207-1246)
+ *   PACKED: depth f32, normal octahedral snorm16x2, color rgba8 unorm,
+ *           params f16x2, motion f16x2                                        */
+#define IRT_GBUFFER_F32 0
+#define IRT_GBUFFER_F16 1
+#define IRT_GBUFFER_PACKED 2
+
+/* Radiance images (noisy lighting, SVGF temporal/scratch/feedback/output):
+ *   F32: f32x4;  F16: f16x4 (the reference's Rgba16Float, src/svgf.rs:23). */
+#define IRT_RADIANCE_F32 0
+#define IRT_RADIANCE_F16 1
+
+/* SVGF moments / history length:
+ *   F32: f32x4 (m1, m2, age, 0) — the reference's Rgba32Float;
+ *   F16: f16x4 (m1, variance, age, 0) — compensated: the variance is kept
+ *        instead of E[x^2] so HDR luminance^2 cannot overflow f16.          */
+#define IRT_MOMENTS_F32 0
+#define IRT_MOMENTS_F16 1
+
+/* SDF atlas texel format: F32 (R32Float, src/renderer.rs:820) or F16 with a
+ * per-mesh scale (texel = f16(value / scale), scale in irt_mesh.lo[3]).      */
+#define IRT_SDF_F32 0
+#define IRT_SDF_F16 1
+
+/* ---------------------------------------------------------------------------
+ * Context, scene, session.
+ * ------------------------------------------------------------------------- */
+typedef struct irt_context irt_context;
+typedef struct irt_scene irt_scene;
+typedef struct irt_session irt_session;
+
+typedef struct irt_config {
+    int32_t device;             /* CUDA ordinal                             */
+    uint64_t hbm_budget_bytes;  /* 0 = 90% of the device's free memory      */
+} irt_config;
+
+irt_status irt_context_create(const irt_config* cfg, irt_context** out);
+void irt_context_destroy(irt_context* ctx);
+const char* irt_last_error(const irt_context* ctx);
+/* Bytes of HBM the context's sessions and scenes hold right now. */
+uint64_t irt_context_bytes_in_use(const irt_context* ctx);
+
+/* Immutable scene data: mesh metadata and the SDF atlas (src/renderer.rs:
+ * 776-888).  `atlas` is host memory of atlas_dims[0]*[1]*[2] texels, x
+ * fastest, in `sdf_format`. */
+irt_status irt_scene_create(irt_context* ctx, const irt_mesh* meshes, uint32_t mesh_count,
+                            const void* atlas, const uint32_t atlas_dims[3], int32_t sdf_format,
+                            irt_scene** out);
+/* Per-frame scene data (src/renderer.rs:1738-1782): objects, preorder BVH
+ * nodes (node_count must be 2*object_count-1) and lights, copied from host
+ * memory on `stream`.  Validates every index the kernels follow. */
+irt_status irt_scene_update(irt_scene* scene, const irt_object* objects, uint32_t object_count,
+                            const irt_node* nodes, uint32_t node_count, const irt_light* lights,
+                            uint32_t light_count, void* stream);
+void irt_scene_destroy(irt_scene* scene);
+
+typedef struct irt_session_desc {
+    irt_settings settings;
+    int32_t gbuffer_format;
+    int32_t radiance_format;
+    int32_t moments_format;
+    int32_t fused;            /* 1 = fused kernels (default), 0 = one kernel per reference entry point */
+    int32_t keep_candidates;  /* 1 = also write the candidates reservoirs [0] (parity/debug) */
+} irt_session_desc;
+
+/* Allocates the session's persistent history (reservoirs, VPL archive, SVGF
+ * targets, previous depth/normal).  Returns IRT_E_ADMISSION when the bytes
+ * would exceed the context's HBM budget. */
+irt_status irt_session_create(irt_context* ctx, const irt_session_desc* desc, irt_session** out);
+/* HBM bytes a session with this description would hold. */
+uint64_t irt_session_bytes(const irt_session_desc* desc);
+void irt_session_destroy(irt_session* s);
+
+typedef struct irt_gbuffer {
+    int32_t format;           /* IRT_GBUFFER_*; must equal the session's     */
+    const float* depth;       /* device pointers, W*H texels each            */
+    const void* normal;
+    const void* color;
+    const void* params;
+    const void* motion;
+} irt_gbuffer;
+
+/* The 8 lighting entry points of lighting.wgsl for one frame, in the order
+ * of src/renderer.rs:1889-1928: VPL archive copy, candidates, temporal,
+ * spatial, resolve.  current/previous VPL pools are caller-owned device
+ * arrays of frame->counts[1] records. */
+irt_status irt_frame_lighting(irt_session* s, const irt_scene* scene, const irt_frame* frame,
+                              const irt_gbuffer* gbuffer, const irt_vpl* current_vpls,
+                              const irt_vpl* previous_vpls, void* stream);
+/* Svgf::encode (src/svgf.rs:140-261) followed by the depth/normal history
+ * copy (src/renderer.rs:1951-1960). */
+irt_status irt_frame_svgf(irt_session* s, const irt_frame* frame, const irt_gbuffer* gbuffer,
+                          void* stream);
+/* Both of the above. */
+irt_status irt_render_frame(irt_session* s, const irt_scene* scene, const irt_frame* frame,
+                            const irt_gbuffer* gbuffer, const irt_vpl* current_vpls,
+                            const irt_vpl* previous_vpls, void* stream);
+
+#define IRT_BUF_DIRECT 0          /* f32x4: resolve_direct output            */
+#define IRT_BUF_NOISY 1           /* radiance fmt: resolve_indirect output   */
+#define IRT_BUF_FILTERED 2        /* radiance fmt: SVGF output of the frame  */
+#define IRT_BUF_MOMENTS 3         /* moments fmt: moments written this frame */
+#define IRT_BUF_RES_DIRECT 4      /* irt_reservoir[3][W*H] ([0],[1],[2])     */
+#define IRT_BUF_RES_INDIRECT 5    /* irt_reservoir[3][W*H]                   */
+#define IRT_BUF_VPL_ARCHIVE 6     /* irt_vpl[(max_history+1)*vpl_count]      */
+#define IRT_BUF_PREV_DEPTH 7      /* f32                                     */
+#define IRT_BUF_PREV_NORMAL 8     /* G-buffer normal format                  */
+#define IRT_BUF_MOMENTS_OLD 9     /* moments slot the next frame reads       */
+#define IRT_BUF_FEEDBACK 10       /* radiance fmt: a-trous-0 output (this)   */
+#define IRT_BUF_FEEDBACK_OLD 11   /* radiance fmt: feedback the next frame reads */
+#define IRT_BUF_ERROR 12          /* u32[4]: device error word (0 = none)    */
+/* Device pointer and byte size of one session buffer.  "This frame" refers
+ * to the last frame submitted. */
+irt_status irt_session_buffer(irt_session* s, int32_t which, void** ptr, uint64_t* bytes);
+/* Reservoir set k (0 = candidates, 1 = temporal, 2 = spatial/final) of a
+ * domain (0 = direct, 1 = indirect): W*H irt_reservoir records.  Set 0 exists
+ * only for unfused sessions or with keep_candidates. */
+irt_status irt_session_reservoirs(irt_session* s, int32_t domain, int32_t k, void** ptr, uint64_t* bytes);
+/* Reads and clears the device error word (bounded-loop violations); returns
+ * IRT_E_DEVICE if a kernel reported one.  Synchronises `stream`. */
+irt_status irt_session_check(irt_session* s, void* stream);
+/* Device time of the last frame's passes (ms), measured with CUDA events
+ * when profiling is on: names as in src/renderer.rs:2077-2092. */
+irt_status irt_session_set_profiling(irt_session* s, int32_t on);
+/* Stages: archive copy, candidates+temporal, spatial+resolve, SVGF temporal,
+ * SVGF variance, a-trous, history copy, total.  Events are kept for the last
+ * 128 frames, so a timed run is read back after it ends. */
+irt_status irt_session_pass_ms(irt_session* s, float out_ms[8]);
+irt_status irt_session_pass_ms_at(irt_session* s, uint32_t frame_index, float out_ms[8]);
+
+/* ---------------------------------------------------------------------------
+ * Host logic of src/renderer.rs used to build scene data (C++ equivalents).
+ * ------------------------------------------------------------------------- */
+/* is_box_geometry (src/renderer.rs:287-329). */
+int32_t irt_is_box_geometry(const irt_vertex* vertices, uint32_t vertex_count,
+                            const uint32_t* indices, uint32_t index_count,
+                            const float lo[3], const float hi[3]);
+/* field_lipschitz_bound (src/renderer.rs:330-358). */
+float irt_field_lipschitz_bound(const float* samples, uint32_t resolution, const float spacing[3]);
+/* Mesh metadata row of Renderer::new (src/renderer.rs:835-885): fills one
+ * irt_mesh from geometry, SDF bounds and samples and its atlas origin. */
+irt_status irt_mesh_metadata(const irt_vertex* vertices, uint32_t vertex_count,
+                             const uint32_t* indices, uint32_t index_count, const float* samples,
+                             uint32_t resolution, const float bounds_min[3],
+                             const float bounds_max[3], const uint32_t atlas_origin[3],
+                             irt_mesh* out);
+/* Atlas tiling of Renderer::new (src/renderer.rs:778-795): tile grid and
+ * extent for `count` meshes of max resolution `tile`. */
+void irt_atlas_layout(uint32_t count, uint32_t tile, uint32_t grid_out[3], uint32_t extent_out[3]);
+/* hierarchy() (src/renderer.rs:385-455): preorder median-split BVH over the
+ * world AABBs of the objects' SDF bounds; writes 2*count-1 nodes. */
+irt_status irt_build_hierarchy(const float* object_lo, const float* object_hi, uint32_t count,
+                               irt_node* nodes_out);
+/* objects() (src/renderer.rs:359-384) for one object. */
+void irt_pack_object(const irt_mat4* model, const irt_mat4* previous, uint32_t mesh_id,
+                     uint32_t material_id, const float sdf_lo[3], const float sdf_hi[3],
+                     uint32_t sdf_resolution, irt_object* out);
+
+/* ---------------------------------------------------------------------------
+ * Synthetic workloads (seeded procedural rooms) and input producers: the
+ * G-buffer producer that stands in for gbuffer.wgsl's raster and the VPL
+ * generator that stands in for vpl.wgsl's ray queries.
+ * ------------------------------------------------------------------------- */
+typedef struct irt_workload_spec {
+    uint64_t seed;
+    uint32_t width, height;
+    uint32_t n_boxes, n_spheres;
+    int32_t room_single_mesh;     /* 1: the six wall slabs are one field mesh */
+    uint32_t sdf_resolution;
+    int32_t sdf_format;           /* IRT_SDF_*                                 */
+    uint32_t n_lights;
+    float radiance_lo, radiance_hi, emitter_size_lo, emitter_size_hi;
+    uint32_t vpl_count, vpl_bounces;
+    float orbit_deg_per_frame, dolly_m_per_frame;
+} irt_workload_spec;
+
+typedef struct irt_workload irt_workload;
+/* Fills spec with config `which` (0: 256x160 room of 12 meshes, 64^3;
+ * 1: 1920x1200 room of 24 meshes, 128^3, 8 emitters, 1024 VPLs). */
+irt_status irt_workload_preset(int32_t which, irt_workload_spec* spec);
+irt_status irt_workload_create(const irt_workload_spec* spec, irt_workload** out);
+void irt_workload_destroy(irt_workload* wl);
+uint32_t irt_workload_mesh_count(const irt_workload* wl);
+uint32_t irt_workload_object_count(const irt_workload* wl);
+uint32_t irt_workload_light_count(const irt_workload* wl);
+const irt_mesh* irt_workload_meshes(const irt_workload* wl);
+const void* irt_workload_atlas(const irt_workload* wl, uint32_t dims_out[3]);
+int32_t irt_workload_sdf_format(const irt_workload* wl);
+/* Settings of the workload (settings.json with the spec's size and VPLs). */
+void irt_workload_settings(const irt_workload* wl, irt_settings* out);
+/* Per-frame scene data and Frame uniform for frame `index` (camera path,
+ * objects with previous transforms, BVH, lights), packed as in
+ * Renderer::encode (src/renderer.rs:1687-1782).  `debug` is the debug mode. */
+irt_status irt_workload_frame(irt_workload* wl, uint32_t index, uint32_t debug, irt_frame* frame,
+                              irt_object* objects, irt_node* nodes, irt_light* lights);
+/* CPU G-buffer producer (analytic primary rays), writing the host planes of
+ * `format` (see IRT_GBUFFER_*): depth, normal, color, params, motion. */
+irt_status irt_workload_gbuffer_cpu(const irt_workload* wl, const irt_frame* frame,
+                                    const irt_object* objects, int32_t format, float* depth,
+                                    void* normal, void* color, void* params, void* motion);
+/* CPU VPL generator: vpl.wgsl:1-47 with analytic ray casts. */
+irt_status irt_workload_vpls_cpu(const irt_workload* wl, const irt_frame* frame,
+                                 const irt_object* objects, const irt_light* lights,
+                                 irt_vpl* out);
+/* CUDA G-buffer producer: same contract as the CPU one, device planes. */
+irt_status irt_gbuffer_render(irt_context* ctx, const irt_workload* wl, const irt_frame* frame,
+                              const irt_object* objects, int32_t format, float* depth,
+                              void* normal, void* color, void* params, void* motion,
+                              void* stream);
+
+#ifdef __cplusplus
+}
+#endif
+#endif /* IRT_H */

@@ -1,0 +1,680 @@
+// capi.cu — the irt_* C-ABI: context, scene and session objects and the
+// per-frame pass schedule of Renderer::encode (src/renderer.rs:1873-1960) and
+// Svgf::encode (src/svgf.rs:140-261).  No exception crosses the boundary.
+#include <cuda_runtime.h>
+
+#include <atomic>
+#include <cstdio>
+#include <cstring>
+#include <mutex>
+#include <new>
+#include <string>
+#include <vector>
+
+#include "kernels.h"
+#include "workload.h"
+
+struct irt_context {
+    int device = 0;
+    uint64_t budget = 0;
+    std::atomic<uint64_t> in_use{0};
+    mutable std::mutex mu;
+    std::string last_error;
+    void set_error(const std::string& e) {
+        std::lock_guard<std::mutex> g(mu);
+        last_error = e;
+    }
+};
+
+struct irt_scene {
+    irt_context* ctx = nullptr;
+    uint32_t mesh_count = 0;
+    irt_mesh* meshes = nullptr;
+    cudaArray_t atlas_array = nullptr;
+    cudaTextureObject_t atlas = 0;
+    int sdf_f16 = 0;
+    uint32_t atlas_dims[3] = {0, 0, 0};
+    std::vector<irt_mesh> host_meshes;
+    // per-frame data
+    irt_object* objects = nullptr;
+    irt_node* nodes = nullptr;
+    irt_light* lights = nullptr;
+    uint32_t object_cap = 0, light_cap = 0;
+    uint32_t object_count = 0, light_count = 0;
+    uint64_t bytes = 0;
+};
+
+struct irt_session {
+    irt_context* ctx = nullptr;
+    irt_session_desc desc{};
+    uint32_t W = 0, H = 0;
+    size_t P = 0;
+    size_t rad_bytes = 0, normal_bytes = 0;
+    irt_reservoir* dres[3] = {nullptr, nullptr, nullptr};
+    irt_reservoir* ires[3] = {nullptr, nullptr, nullptr};
+    irt_vpl* archive = nullptr;
+    float* prev_depth = nullptr;
+    void* prev_normal = nullptr;
+    float4* direct = nullptr;
+    void* noisy = nullptr;
+    float4* moments[2] = {nullptr, nullptr};
+    void* feedback[2] = {nullptr, nullptr};
+    void* temporal = nullptr;
+    void* scratch[2] = {nullptr, nullptr};
+    void* filtered = nullptr;
+    uint32_t* error = nullptr;
+    uint64_t bytes = 0;
+    uint32_t last_frame = 0;
+    bool have_frame = false;
+    bool profiling = false;
+    // Profiling: a ring of kProfRing frames x 8 stage-boundary events, so a
+    // long timed run can be read back afterwards without per-frame syncs.
+    static constexpr int kProfRing = 128;
+    cudaEvent_t ev[kProfRing][8] = {};
+    bool ev_ready = false;
+    int prof_slot = 0;
+    uint32_t prof_frame[kProfRing] = {};
+};
+
+namespace {
+
+uint32_t normal_bytes_of(int fmt) {
+    return fmt == IRT_GBUFFER_F32 ? 16u : (fmt == IRT_GBUFFER_F16 ? 8u : 4u);
+}
+
+irt_status cuda_fail(irt_context* ctx, cudaError_t e, const char* what) {
+    if (ctx) ctx->set_error(std::string(what) + ": " + cudaGetErrorString(e));
+    return IRT_E_CUDA;
+}
+
+#define CK(call, what)                                   \
+    do {                                                 \
+        cudaError_t _e = (call);                         \
+        if (_e != cudaSuccess) return cuda_fail(ctx, _e, what); \
+    } while (0)
+
+struct DeviceGuard {
+    int prev = -1;
+    explicit DeviceGuard(int dev) {
+        if (cudaGetDevice(&prev) != cudaSuccess) prev = -1;
+        if (prev != dev) cudaSetDevice(dev);
+    }
+    ~DeviceGuard() {
+        int cur = -1;
+        if (prev >= 0 && cudaGetDevice(&cur) == cudaSuccess && cur != prev) cudaSetDevice(prev);
+    }
+};
+
+template <class T>
+irt_status dev_alloc(irt_context* ctx, T** p, size_t bytes, uint64_t& counter) {
+    if (bytes == 0) {
+        *p = nullptr;
+        return IRT_OK;
+    }
+    void* q = nullptr;
+    cudaError_t e = cudaMalloc(&q, bytes);
+    if (e != cudaSuccess) return cuda_fail(ctx, e, "cudaMalloc");
+    e = cudaMemset(q, 0, bytes);
+    if (e != cudaSuccess) {
+        cudaFree(q);
+        return cuda_fail(ctx, e, "cudaMemset");
+    }
+    *p = static_cast<T*>(q);
+    counter += bytes;
+    return IRT_OK;
+}
+
+bool needs_candidates(const irt_session_desc& d) { return d.keep_candidates || !d.fused; }
+
+}  // namespace
+
+extern "C" {
+
+// ------------------------------------------------------------------ context
+irt_status irt_context_create(const irt_config* cfg, irt_context** out) {
+    if (!out) return IRT_E_INVALID;
+    *out = nullptr;
+    int count = 0;
+    if (cudaGetDeviceCount(&count) != cudaSuccess || count == 0) {
+        cudaGetLastError();
+        return IRT_E_NODEVICE;
+    }
+    int dev = cfg ? cfg->device : 0;
+    if (dev < 0 || dev >= count) return IRT_E_INVALID;
+    irt_context* ctx = new (std::nothrow) irt_context();
+    if (!ctx) return IRT_E_NOMEM;
+    ctx->device = dev;
+    DeviceGuard g(dev);
+    size_t free_b = 0, total_b = 0;
+    if (cudaMemGetInfo(&free_b, &total_b) != cudaSuccess) {
+        delete ctx;
+        return IRT_E_CUDA;
+    }
+    ctx->budget = (cfg && cfg->hbm_budget_bytes) ? cfg->hbm_budget_bytes : (uint64_t)(free_b * 0.9);
+    *out = ctx;
+    return IRT_OK;
+}
+
+void irt_context_destroy(irt_context* ctx) { delete ctx; }
+
+const char* irt_last_error(const irt_context* ctx) {
+    if (!ctx) return "null context";
+    std::lock_guard<std::mutex> g(ctx->mu);
+    return ctx->last_error.c_str();
+}
+
+uint64_t irt_context_bytes_in_use(const irt_context* ctx) { return ctx ? ctx->in_use.load() : 0; }
+
+// ------------------------------------------------------------------ scene
+irt_status irt_scene_create(irt_context* ctx, const irt_mesh* meshes, uint32_t mesh_count, const void* atlas,
+                            const uint32_t atlas_dims[3], int32_t sdf_format, irt_scene** out) {
+    if (!ctx || !out || !meshes || mesh_count == 0 || !atlas || !atlas_dims) return IRT_E_INVALID;
+    if (sdf_format != IRT_SDF_F32 && sdf_format != IRT_SDF_F16) return IRT_E_INVALID;
+    *out = nullptr;
+    // Every texel a mesh can address must lie inside the atlas.
+    for (uint32_t m = 0; m < mesh_count; m++) {
+        const irt_mesh& me = meshes[m];
+        if (me.geometry_lo[3] > .5f) continue;
+        uint32_t res = me.field[3];
+        if (res < 2) {
+            ctx->set_error("mesh resolution below 2");
+            return IRT_E_INVALID;
+        }
+        for (int a = 0; a < 3; a++)
+            if ((uint64_t)me.field[a] + res > atlas_dims[a]) {
+                ctx->set_error("mesh field tile outside the atlas");
+                return IRT_E_INVALID;
+            }
+    }
+    DeviceGuard g(ctx->device);
+    irt_scene* sc = new (std::nothrow) irt_scene();
+    if (!sc) return IRT_E_NOMEM;
+    sc->ctx = ctx;
+    sc->mesh_count = mesh_count;
+    sc->sdf_f16 = sdf_format == IRT_SDF_F16;
+    for (int a = 0; a < 3; a++) sc->atlas_dims[a] = atlas_dims[a];
+    sc->host_meshes.assign(meshes, meshes + mesh_count);
+    auto fail = [&](irt_status s) {
+        irt_scene_destroy(sc);
+        return s;
+    };
+    irt_status st = dev_alloc(ctx, &sc->meshes, sizeof(irt_mesh) * mesh_count, sc->bytes);
+    if (st) return fail(st);
+    cudaError_t e = cudaMemcpy(sc->meshes, meshes, sizeof(irt_mesh) * mesh_count, cudaMemcpyHostToDevice);
+    if (e != cudaSuccess) return fail(cuda_fail(ctx, e, "mesh upload"));
+    cudaChannelFormatDesc cd =
+        sdf_format == IRT_SDF_F16 ? cudaCreateChannelDescHalf() : cudaCreateChannelDesc<float>();
+    cudaExtent ext = make_cudaExtent(atlas_dims[0], atlas_dims[1], atlas_dims[2]);
+    e = cudaMalloc3DArray(&sc->atlas_array, &cd, ext);
+    if (e != cudaSuccess) return fail(cuda_fail(ctx, e, "cudaMalloc3DArray"));
+    size_t texel = sdf_format == IRT_SDF_F16 ? 2 : 4;
+    sc->bytes += texel * atlas_dims[0] * atlas_dims[1] * (size_t)atlas_dims[2];
+    cudaMemcpy3DParms cp{};
+    cp.srcPtr = make_cudaPitchedPtr(const_cast<void*>(atlas), atlas_dims[0] * texel, atlas_dims[0], atlas_dims[1]);
+    cp.dstArray = sc->atlas_array;
+    cp.extent = ext;
+    cp.kind = cudaMemcpyHostToDevice;
+    e = cudaMemcpy3D(&cp);
+    if (e != cudaSuccess) return fail(cuda_fail(ctx, e, "atlas upload"));
+    cudaResourceDesc rd{};
+    rd.resType = cudaResourceTypeArray;
+    rd.res.array.array = sc->atlas_array;
+    cudaTextureDesc td{};
+    td.addressMode[0] = td.addressMode[1] = td.addressMode[2] = cudaAddressModeClamp;
+    td.filterMode = cudaFilterModePoint;
+    td.readMode = cudaReadModeElementType;
+    td.normalizedCoords = 0;
+    e = cudaCreateTextureObject(&sc->atlas, &rd, &td, nullptr);
+    if (e != cudaSuccess) return fail(cuda_fail(ctx, e, "texture object"));
+    ctx->in_use += sc->bytes;
+    *out = sc;
+    return IRT_OK;
+}
+
+irt_status irt_scene_update(irt_scene* sc, const irt_object* objects, uint32_t object_count, const irt_node* nodes,
+                            uint32_t node_count, const irt_light* lights, uint32_t light_count, void* stream) {
+    if (!sc) return IRT_E_INVALID;
+    irt_context* ctx = sc->ctx;
+    if (!objects || object_count == 0 || !nodes || node_count != 2 * object_count - 1 || (light_count && !lights)) {
+        ctx->set_error("scene update needs objects and 2N-1 nodes");
+        return IRT_E_INVALID;
+    }
+    // Validate every index the device walk follows: mesh ids, leaf object
+    // ids, and escape links that strictly advance and stay within 2N-1.
+    for (uint32_t i = 0; i < object_count; i++)
+        if (objects[i].info[0] >= sc->mesh_count) {
+            ctx->set_error("object references a mesh outside the scene");
+            return IRT_E_INVALID;
+        }
+    for (uint32_t i = 0; i < node_count; i++) {
+        const irt_node& n = nodes[i];
+        if (n.info[3] <= i || n.info[3] > node_count || (n.info[2] == 1u && n.info[0] >= object_count)) {
+            ctx->set_error("malformed BVH node");
+            return IRT_E_INVALID;
+        }
+    }
+    DeviceGuard g(ctx->device);
+    cudaStream_t st = static_cast<cudaStream_t>(stream);
+    if (object_count > sc->object_cap) {
+        uint64_t before = sc->bytes;
+        if (sc->objects) cudaFree(sc->objects);
+        if (sc->nodes) cudaFree(sc->nodes);
+        sc->objects = nullptr;
+        sc->nodes = nullptr;
+        uint64_t added = 0;
+        irt_status s1 = dev_alloc(ctx, &sc->objects, sizeof(irt_object) * object_count, added);
+        if (s1) return s1;
+        s1 = dev_alloc(ctx, &sc->nodes, sizeof(irt_node) * (2 * (size_t)object_count - 1), added);
+        if (s1) return s1;
+        sc->object_cap = object_count;
+        sc->bytes = before + added;
+        ctx->in_use += added;
+    }
+    if (light_count > sc->light_cap) {
+        if (sc->lights) cudaFree(sc->lights);
+        sc->lights = nullptr;
+        uint64_t added = 0;
+        irt_status s1 = dev_alloc(ctx, &sc->lights, sizeof(irt_light) * light_count, added);
+        if (s1) return s1;
+        sc->light_cap = light_count;
+        sc->bytes += added;
+        ctx->in_use += added;
+    }
+    CK(cudaMemcpyAsync(sc->objects, objects, sizeof(irt_object) * object_count, cudaMemcpyHostToDevice, st), "objects");
+    CK(cudaMemcpyAsync(sc->nodes, nodes, sizeof(irt_node) * node_count, cudaMemcpyHostToDevice, st), "nodes");
+    if (light_count)
+        CK(cudaMemcpyAsync(sc->lights, lights, sizeof(irt_light) * light_count, cudaMemcpyHostToDevice, st), "lights");
+    sc->object_count = object_count;
+    sc->light_count = light_count;
+    return IRT_OK;
+}
+
+void irt_scene_destroy(irt_scene* sc) {
+    if (!sc) return;
+    DeviceGuard g(sc->ctx->device);
+    if (sc->atlas) cudaDestroyTextureObject(sc->atlas);
+    if (sc->atlas_array) cudaFreeArray(sc->atlas_array);
+    if (sc->meshes) cudaFree(sc->meshes);
+    if (sc->objects) cudaFree(sc->objects);
+    if (sc->nodes) cudaFree(sc->nodes);
+    if (sc->lights) cudaFree(sc->lights);
+    if (sc->ctx->in_use >= sc->bytes) sc->ctx->in_use -= sc->bytes;
+    delete sc;
+}
+
+// ------------------------------------------------------------------ session
+uint64_t irt_session_bytes(const irt_session_desc* d) {
+    if (!d) return 0;
+    uint64_t P = (uint64_t)d->settings.render_width * d->settings.render_height;
+    uint64_t rad = d->radiance_format == IRT_RADIANCE_F16 ? 8 : 16;
+    uint64_t res_sets = needs_candidates(*d) ? 3 : 2;
+    uint64_t b = 0;
+    b += 2 * res_sets * P * 32;                                                     // reservoirs
+    b += (uint64_t)(d->settings.restir_max_history + 1) * d->settings.vpl_count * 48;  // archive
+    b += P * 4 + P * normal_bytes_of(d->gbuffer_format);                            // previous depth/normal
+    b += P * 16;                                                                    // direct f32x4
+    b += P * rad * 7;  // noisy, feedback x2, temporal, scratch x2, filtered
+    b += P * 16 * 2;   // moments x2
+    b += 16;           // error word
+    return b;
+}
+
+irt_status irt_session_create(irt_context* ctx, const irt_session_desc* desc, irt_session** out) {
+    if (!ctx || !desc || !out) return IRT_E_INVALID;
+    *out = nullptr;
+    char msg[128];
+    if (irt_settings_validate(&desc->settings, msg, sizeof(msg)) != IRT_OK) {
+        ctx->set_error(msg);
+        return IRT_E_INVALID;
+    }
+    if (desc->gbuffer_format < IRT_GBUFFER_F32 || desc->gbuffer_format > IRT_GBUFFER_PACKED ||
+        (desc->radiance_format != IRT_RADIANCE_F32 && desc->radiance_format != IRT_RADIANCE_F16) ||
+        desc->moments_format != IRT_MOMENTS_F32) {
+        ctx->set_error("unsupported storage format");
+        return IRT_E_INVALID;
+    }
+    uint64_t need = irt_session_bytes(desc);
+    // Admission by HBM bytes against the context budget.
+    uint64_t cur = ctx->in_use.load();
+    for (;;) {
+        if (cur + need > ctx->budget) {
+            ctx->set_error("session exceeds the HBM budget");
+            return IRT_E_ADMISSION;
+        }
+        if (ctx->in_use.compare_exchange_weak(cur, cur + need)) break;
+    }
+    DeviceGuard g(ctx->device);
+    irt_session* s = new (std::nothrow) irt_session();
+    if (!s) {
+        ctx->in_use -= need;
+        return IRT_E_NOMEM;
+    }
+    s->ctx = ctx;
+    s->desc = *desc;
+    s->W = desc->settings.render_width;
+    s->H = desc->settings.render_height;
+    s->P = (size_t)s->W * s->H;
+    s->rad_bytes = desc->radiance_format == IRT_RADIANCE_F16 ? 8 : 16;
+    s->normal_bytes = normal_bytes_of(desc->gbuffer_format);
+    s->bytes = need;
+    uint64_t used = 0;
+    auto fail = [&](irt_status st) {
+        irt_session_destroy(s);
+        return st;
+    };
+    const size_t P = s->P;
+    for (int k = needs_candidates(*desc) ? 0 : 1; k < 3; k++) {
+        irt_status st = dev_alloc(ctx, &s->dres[k], P * 32, used);
+        if (st) return fail(st);
+        st = dev_alloc(ctx, &s->ires[k], P * 32, used);
+        if (st) return fail(st);
+    }
+    irt_status st = dev_alloc(ctx, &s->archive,
+                              (size_t)(desc->settings.restir_max_history + 1) * desc->settings.vpl_count * 48, used);
+    if (!st) st = dev_alloc(ctx, &s->prev_depth, P * 4, used);
+    if (!st) st = dev_alloc(ctx, &s->prev_normal, P * s->normal_bytes, used);
+    if (!st) st = dev_alloc(ctx, &s->direct, P * 16, used);
+    if (!st) st = dev_alloc(ctx, &s->noisy, P * s->rad_bytes, used);
+    for (int k = 0; k < 2 && !st; k++) {
+        st = dev_alloc(ctx, &s->moments[k], P * 16, used);
+        if (!st) st = dev_alloc(ctx, &s->feedback[k], P * s->rad_bytes, used);
+        if (!st) st = dev_alloc(ctx, &s->scratch[k], P * s->rad_bytes, used);
+    }
+    if (!st) st = dev_alloc(ctx, &s->temporal, P * s->rad_bytes, used);
+    if (!st) st = dev_alloc(ctx, &s->filtered, P * s->rad_bytes, used);
+    if (!st) st = dev_alloc(ctx, &s->error, 16, used);
+    if (st) return fail(st);
+    *out = s;
+    return IRT_OK;
+}
+
+void irt_session_destroy(irt_session* s) {
+    if (!s) return;
+    DeviceGuard g(s->ctx->device);
+    void* ptrs[] = {s->dres[0], s->dres[1], s->dres[2], s->ires[0], s->ires[1], s->ires[2], s->archive,
+                    s->prev_depth, s->prev_normal, s->direct, s->noisy, s->moments[0], s->moments[1],
+                    s->feedback[0], s->feedback[1], s->temporal, s->scratch[0], s->scratch[1], s->filtered, s->error};
+    for (void* p : ptrs)
+        if (p) cudaFree(p);
+    if (s->ev_ready)
+        for (auto& row : s->ev)
+            for (cudaEvent_t e : row) cudaEventDestroy(e);
+    if (s->ctx->in_use >= s->bytes) s->ctx->in_use -= s->bytes;
+    delete s;
+}
+
+static irt_status check_frame(irt_session* s, const irt_frame* f, const irt_gbuffer* g) {
+    irt_context* ctx = s->ctx;
+    if (!f || !g) return IRT_E_INVALID;
+    if (f->size[0] != s->W || f->size[1] != s->H) {
+        ctx->set_error("frame size differs from the session's");
+        return IRT_E_INVALID;
+    }
+    if (g->format != s->desc.gbuffer_format || !g->depth || !g->normal || !g->color || !g->params || !g->motion) {
+        ctx->set_error("G-buffer format or planes invalid");
+        return IRT_E_INVALID;
+    }
+    return IRT_OK;
+}
+
+static void mark(irt_session* s, int k, cudaStream_t st) {
+    if (s->profiling && s->ev_ready) cudaEventRecord(s->ev[s->prof_slot][k], st);
+}
+
+irt_status irt_frame_lighting(irt_session* s, const irt_scene* sc, const irt_frame* f, const irt_gbuffer* g,
+                              const irt_vpl* cur, const irt_vpl* prev, void* stream) {
+    if (!s || !sc) return IRT_E_INVALID;
+    irt_context* ctx = s->ctx;
+    irt_status chk = check_frame(s, f, g);
+    if (chk) return chk;
+    const irt_settings& set = s->desc.settings;
+    if (f->counts[1] != set.vpl_count || f->counts[3] != sc->object_count || f->counts[0] > sc->light_count) {
+        ctx->set_error("frame counts differ from the session/scene");
+        return IRT_E_INVALID;
+    }
+    // Loop bounds the kernels take from the frame stay within the ranges
+    // Settings::validate admits (src/settings.rs:63-94).
+    if (f->restir[0] == 0 || f->restir[0] > 256 || f->restir[1] == 0 || f->restir[1] > 256 || f->restir[2] > 32 ||
+        f->restir[3] > 256 || !(f->sdf[0] >= 1.f && f->sdf[0] <= 1024.f) || !(f->sdf[1] > 0.f)) {
+        ctx->set_error("frame ReSTIR/SDF parameters out of range");
+        return IRT_E_INVALID;
+    }
+    if (!cur || !prev) {
+        ctx->set_error("VPL pools required");
+        return IRT_E_INVALID;
+    }
+    if ((uint32_t)f->rr[2] != set.restir_max_history) {
+        ctx->set_error("frame rr.z differs from restir_max_history");
+        return IRT_E_INVALID;
+    }
+    DeviceGuard dg(ctx->device);
+    cudaStream_t st = static_cast<cudaStream_t>(stream);
+    s->prof_slot = (int)(f->size[2] % irt_session::kProfRing);
+    s->prof_frame[s->prof_slot] = f->size[2];
+    mark(s, 0, st);
+    // VPL archive ring slot frame % (H+1) (src/renderer.rs:1873-1884).
+    size_t pool = (size_t)set.vpl_count * sizeof(irt_vpl);
+    uint32_t slot = f->size[2] % (set.restir_max_history + 1u);
+    CK(cudaMemcpyAsync((char*)s->archive + slot * pool, cur, pool, cudaMemcpyDeviceToDevice, st), "archive copy");
+    mark(s, 1, st);
+    LightingLaunch L{};
+    L.frame = f;
+    L.gbuffer = *g;
+    L.objects = sc->objects;
+    L.meshes = sc->meshes;
+    L.nodes = sc->nodes;
+    L.lights = sc->lights;
+    L.atlas = sc->atlas;
+    L.sdf_f16 = sc->sdf_f16;
+    L.error = s->error;
+    L.cur_vpls = cur;
+    L.prev_vpls = prev;
+    L.archive = s->archive;
+    L.prev_depth = s->prev_depth;
+    L.prev_normal = s->prev_normal;
+    for (int k = 0; k < 3; k++) {
+        L.dres[k] = s->dres[k];
+        L.ires[k] = s->ires[k];
+    }
+    L.direct_out = s->direct;
+    L.noisy_out = s->noisy;
+    L.radiance_f16 = s->desc.radiance_format == IRT_RADIANCE_F16;
+    L.keep_candidates = s->desc.keep_candidates;
+    if (s->desc.fused) {
+        CK(irt_launch_lighting(L, kStageReuse, st), "reuse kernel");
+        mark(s, 2, st);
+        CK(irt_launch_lighting(L, kStageShade, st), "shade kernel");
+        mark(s, 3, st);
+    } else {
+        for (int p = 0; p < 4; p++) CK(irt_launch_lighting(L, p, st), "lighting pass");
+        mark(s, 2, st);
+        for (int p = 4; p < 8; p++) CK(irt_launch_lighting(L, p, st), "lighting pass");
+        mark(s, 3, st);
+    }
+    s->last_frame = f->size[2];
+    s->have_frame = true;
+    return IRT_OK;
+}
+
+irt_status irt_frame_svgf(irt_session* s, const irt_frame* f, const irt_gbuffer* g, void* stream) {
+    if (!s) return IRT_E_INVALID;
+    irt_context* ctx = s->ctx;
+    irt_status chk = check_frame(s, f, g);
+    if (chk) return chk;
+    DeviceGuard dg(ctx->device);
+    cudaStream_t st = static_cast<cudaStream_t>(stream);
+    const int cur = (int)(f->size[2] % 2u), old = 1 - cur;
+    const size_t rb = s->P * s->rad_bytes;
+    if (f->flags[2] >= 3u) {  // debug views bypass SVGF (src/svgf.rs:154-161)
+        CK(cudaMemcpyAsync(s->filtered, s->noisy, rb, cudaMemcpyDeviceToDevice, st), "svgf bypass");
+        mark(s, 4, st);
+        mark(s, 5, st);
+        mark(s, 6, st);
+    } else {
+        SvgfLaunch L{};
+        L.frame = f;
+        L.gbuffer = *g;
+        L.old_depth = s->prev_depth;
+        L.old_normal = s->prev_normal;
+        L.radiance_f16 = s->desc.radiance_format == IRT_RADIANCE_F16;
+        L.in = s->noisy;
+        L.aux = s->feedback[old];
+        L.moments_in = s->moments[old];
+        L.out = s->temporal;
+        L.moments_out = s->moments[cur];
+        CK(irt_launch_svgf(L, 0, st), "svgf temporal");
+        mark(s, 4, st);
+        L.in = s->temporal;
+        L.moments_in = s->moments[cur];
+        L.out = s->scratch[0];
+        CK(irt_launch_svgf(L, 1, st), "svgf variance");
+        mark(s, 5, st);
+        // A-trous ping-pong: iteration 0 writes feedback[cur] directly (the
+        // reference copies scratch[1] there), the last writes the output.
+        const uint32_t iters = s->desc.settings.svgf_iterations;
+        const void* in = s->scratch[0];
+        for (uint32_t i = 0; i < iters; i++) {
+            void* out;
+            void* out2 = nullptr;
+            if (i + 1 == iters) {
+                out = s->filtered;
+                if (i == 0) out2 = s->feedback[cur];
+            } else {
+                out = i == 0 ? s->feedback[cur] : s->scratch[i % 2];
+            }
+            L.in = in;
+            L.out = out;
+            L.out2 = out2;
+            L.step = 1 << i;
+            CK(irt_launch_svgf(L, 2, st), "svgf atrous");
+            in = out;
+        }
+        mark(s, 6, st);
+    }
+    // Depth/normal history for the next frame (src/renderer.rs:1951-1960).
+    CK(cudaMemcpyAsync(s->prev_depth, g->depth, s->P * 4, cudaMemcpyDeviceToDevice, st), "depth history");
+    CK(cudaMemcpyAsync(s->prev_normal, g->normal, s->P * s->normal_bytes, cudaMemcpyDeviceToDevice, st),
+       "normal history");
+    mark(s, 7, st);
+    return IRT_OK;
+}
+
+irt_status irt_render_frame(irt_session* s, const irt_scene* sc, const irt_frame* f, const irt_gbuffer* g,
+                            const irt_vpl* cur, const irt_vpl* prev, void* stream) {
+    irt_status r = irt_frame_lighting(s, sc, f, g, cur, prev, stream);
+    if (r) return r;
+    return irt_frame_svgf(s, f, g, stream);
+}
+
+irt_status irt_session_buffer(irt_session* s, int32_t which, void** ptr, uint64_t* bytes) {
+    if (!s || !ptr || !bytes) return IRT_E_INVALID;
+    const size_t P = s->P;
+    const int cur = (int)(s->last_frame % 2u), old = 1 - cur;
+    void* p = nullptr;
+    uint64_t b = 0;
+    switch (which) {
+    case IRT_BUF_DIRECT: p = s->direct; b = P * 16; break;
+    case IRT_BUF_NOISY: p = s->noisy; b = P * s->rad_bytes; break;
+    case IRT_BUF_FILTERED: p = s->filtered; b = P * s->rad_bytes; break;
+    case IRT_BUF_MOMENTS: p = s->moments[cur]; b = P * 16; break;
+    case IRT_BUF_MOMENTS_OLD: p = s->moments[old]; b = P * 16; break;
+    case IRT_BUF_FEEDBACK: p = s->feedback[cur]; b = P * s->rad_bytes; break;
+    case IRT_BUF_FEEDBACK_OLD: p = s->feedback[old]; b = P * s->rad_bytes; break;
+    case IRT_BUF_VPL_ARCHIVE:
+        p = s->archive;
+        b = (uint64_t)(s->desc.settings.restir_max_history + 1) * s->desc.settings.vpl_count * 48;
+        break;
+    case IRT_BUF_PREV_DEPTH: p = s->prev_depth; b = P * 4; break;
+    case IRT_BUF_PREV_NORMAL: p = s->prev_normal; b = P * s->normal_bytes; break;
+    case IRT_BUF_ERROR: p = s->error; b = 16; break;
+    default: break;
+    }
+    if (which == IRT_BUF_RES_DIRECT || which == IRT_BUF_RES_INDIRECT) {
+        // Three separate allocations: report [2] (the final reservoirs); [0]
+        // and [1] are reachable through irt_session_reservoirs.
+        irt_reservoir** set = which == IRT_BUF_RES_DIRECT ? s->dres : s->ires;
+        p = set[2];
+        b = P * 32;
+    }
+    if (!p) return IRT_E_INVALID;
+    *ptr = p;
+    *bytes = b;
+    return IRT_OK;
+}
+
+irt_status irt_session_check(irt_session* s, void* stream) {
+    if (!s) return IRT_E_INVALID;
+    irt_context* ctx = s->ctx;
+    DeviceGuard dg(ctx->device);
+    cudaStream_t st = static_cast<cudaStream_t>(stream);
+    uint32_t h[4] = {0, 0, 0, 0};
+    CK(cudaMemcpyAsync(h, s->error, 16, cudaMemcpyDeviceToHost, st), "error word");
+    CK(cudaStreamSynchronize(st), "sync");
+    CK(cudaMemsetAsync(s->error, 0, 16, st), "error clear");
+    if (h[0]) {
+        char buf[96];
+        std::snprintf(buf, sizeof(buf), "device error word 0x%x", h[0]);
+        ctx->set_error(buf);
+        return IRT_E_DEVICE;
+    }
+    return IRT_OK;
+}
+
+irt_status irt_session_set_profiling(irt_session* s, int32_t on) {
+    if (!s) return IRT_E_INVALID;
+    irt_context* ctx = s->ctx;
+    if (on && !s->ev_ready) {
+        DeviceGuard dg(ctx->device);
+        for (auto& row : s->ev)
+            for (cudaEvent_t& e : row) CK(cudaEventCreate(&e), "event");
+        s->ev_ready = true;
+    }
+    s->profiling = on != 0;
+    return IRT_OK;
+}
+
+// Device time of one profiled frame's stages (ms): archive copy, candidates +
+// temporal, spatial + resolve, SVGF temporal, SVGF variance, a-trous,
+// history copy, total.  Synchronises on that frame's last event.  Frames
+// older than the ring (128 frames) are overwritten.
+irt_status irt_session_pass_ms_at(irt_session* s, uint32_t frame_index, float out_ms[8]) {
+    if (!s || !out_ms || !s->ev_ready) return IRT_E_STATE;
+    irt_context* ctx = s->ctx;
+    int slot = (int)(frame_index % irt_session::kProfRing);
+    if (s->prof_frame[slot] != frame_index) {
+        ctx->set_error("frame not in the profiling ring");
+        return IRT_E_STATE;
+    }
+    DeviceGuard dg(ctx->device);
+    cudaEvent_t* e = s->ev[slot];
+    CK(cudaEventSynchronize(e[7]), "event sync");
+    for (int k = 0; k < 7; k++) CK(cudaEventElapsedTime(&out_ms[k], e[k], e[k + 1]), "elapsed");
+    CK(cudaEventElapsedTime(&out_ms[7], e[0], e[7]), "elapsed");
+    return IRT_OK;
+}
+
+irt_status irt_session_pass_ms(irt_session* s, float out_ms[8]) {
+    if (!s) return IRT_E_INVALID;
+    return irt_session_pass_ms_at(s, s->last_frame, out_ms);
+}
+
+// Reservoir set k (0, 1, 2) of a domain (0 direct, 1 indirect).
+irt_status irt_session_reservoirs(irt_session* s, int32_t domain, int32_t k, void** ptr, uint64_t* bytes) {
+    if (!s || !ptr || !bytes || domain < 0 || domain > 1 || k < 0 || k > 2) return IRT_E_INVALID;
+    irt_reservoir* p = domain == 0 ? s->dres[k] : s->ires[k];
+    if (!p) return IRT_E_STATE;
+    *ptr = p;
+    *bytes = s->P * 32;
+    return IRT_OK;
+}
+
+void irt_workload_destroy(irt_workload* wl) {
+    if (!wl) return;
+    if (wl->w.dev_prims) {
+        DeviceGuard g(wl->w.dev_prims_device);
+        cudaFree(wl->w.dev_prims);
+    }
+    delete wl;
+}
+
+}  // extern "C"

@@ -1,0 +1,214 @@
+// dev_sdf.cuh — device restatement of sdf.wgsl: signed distance bounds of
+// meshes (certified boxes exactly, others from the trilinear SDF atlas read
+// through the texture path), the stackless preorder BVH walk with escape links
+// and the Quilez soft-shadow march.
+#pragma once
+#include "dev_common.cuh"
+
+namespace irtd {
+
+struct DevScene {
+    const irt_object* objects;
+    const irt_mesh* meshes;
+    const irt_node* nodes;
+    const irt_light* lights;
+    cudaTextureObject_t atlas;  // 3-D R32F or R16F texels, point sampled
+    int32_t sdf_f16;            // texel = f16(value / mesh.lo[3])
+    uint32_t* error;            // device error word
+};
+
+// Read-only-path loads of the scene records as 16-byte vectors.
+struct DMesh {
+    float4 lo, hi;
+    uint4 field;
+    float4 grid, glo, ghi, sphere;
+};
+__device__ __forceinline__ DMesh load_mesh(const irt_mesh* base, uint32_t i) {
+    const float4* p = reinterpret_cast<const float4*>(base + i);
+    DMesh m;
+    m.lo = __ldg(p);
+    m.hi = __ldg(p + 1);
+    m.field = __ldg(reinterpret_cast<const uint4*>(p + 3));
+    m.grid = __ldg(p + 4);
+    m.glo = __ldg(p + 5);
+    m.ghi = __ldg(p + 6);
+    m.sphere = __ldg(p + 7);
+    return m;
+}
+struct DObject {  // inverse matrix columns and info
+    float4 c0, c1, c2, c3;
+    uint4 info;
+};
+__device__ __forceinline__ DObject load_object(const irt_object* base, uint32_t i) {
+    const float4* p = reinterpret_cast<const float4*>(base + i);
+    DObject o;
+    o.c0 = __ldg(p + 8);
+    o.c1 = __ldg(p + 9);
+    o.c2 = __ldg(p + 10);
+    o.c3 = __ldg(p + 11);
+    o.info = __ldg(reinterpret_cast<const uint4*>(p + 12));
+    return o;
+}
+struct DNode {
+    float4 lo, hi;
+    uint4 info;
+};
+__device__ __forceinline__ DNode load_node(const irt_node* base, uint32_t i) {
+    const float4* p = reinterpret_cast<const float4*>(base + i);
+    return DNode{__ldg(p), __ldg(p + 1), __ldg(reinterpret_cast<const uint4*>(p + 2))};
+}
+
+// sdf.wgsl:1-4
+__device__ __forceinline__ float signed_box_distance(V3 p, V3 lo, V3 hi) {
+    V3 delta = vmax(lo - p, p - hi);
+    return length(vmax(delta, V3{0.f, 0.f, 0.f})) + wmin(wmax(delta.x, wmax(delta.y, delta.z)), 0.f);
+}
+
+// common.wgsl:31-38 — 8 texel loads, cell clamped to res-2, weights in
+// z, y, x order as the WGSL loop accumulates them.
+__device__ __forceinline__ float sample_field(const DevScene& sc, const DMesh& m, V3 q) {
+    uint32_t res = m.field.w;
+    uint32_t cx = min(to_u32(floorf(q.x)), res - 2u);
+    uint32_t cy = min(to_u32(floorf(q.y)), res - 2u);
+    uint32_t cz = min(to_u32(floorf(q.z)), res - 2u);
+    float fx = q.x - (float)cx, fy = q.y - (float)cy, fz = q.z - (float)cz;
+    float bx = (float)(m.field.x + cx) + 0.5f;
+    float by = (float)(m.field.y + cy) + 0.5f;
+    float bz = (float)(m.field.z + cz) + 0.5f;
+    float t[8];
+#pragma unroll
+    for (int k = 0; k < 8; k++)
+        t[k] = tex3D<float>(sc.atlas, bx + (float)(k & 1), by + (float)((k >> 1) & 1), bz + (float)(k >> 2));
+    if (sc.sdf_f16) {
+        float s = m.lo.w;
+#pragma unroll
+        for (int k = 0; k < 8; k++) t[k] *= s;
+    }
+    float value = 0.f;
+#pragma unroll
+    for (int k = 0; k < 8; k++) {
+        float wx = (k & 1) ? fx : 1.f - fx;
+        float wy = ((k >> 1) & 1) ? fy : 1.f - fy;
+        float wz = (k >> 2) ? fz : 1.f - fz;
+        value += t[k] * wx * wy * wz;
+    }
+    return value;
+}
+
+// sdf.wgsl:5-33
+__device__ __forceinline__ float mesh_distance(const DevScene& sc, V3 p, const DMesh& m) {
+    float geometry_bound = signed_box_distance(p, xyz(m.glo), xyz(m.ghi));
+    if (m.glo.w > .5f) return geometry_bound;
+    V3 lo = xyz(m.lo), hi = xyz(m.hi);
+    V3 clamped = vmin(vmax(p, lo), hi);
+    V3 q = (clamped - lo) * xyz(m.grid);
+    float value = sample_field(sc, m, q);
+    float bound = value - m.grid.w * (.5f + 1.f / 128.f);
+    V3 outside = vmax(vmax(lo - p, p - hi), V3{0.f, 0.f, 0.f});
+    float os = dot(outside, outside);
+    if (os > 0.f) {
+        float positive = wmax(bound, 0.f);
+        bound = sqrtf(positive * positive + os);
+    }
+    if (bound > 0.f) bound *= m.ghi.w;
+    float sphere_bound = length(p - xyz(m.sphere)) - m.sphere.w;
+    return wmax(bound, wmax(geometry_bound, sphere_bound));
+}
+
+// sdf.wgsl:35-41 (returns the distance; the voxel is selected by the caller).
+__device__ __forceinline__ float object_distance(const DevScene& sc, V3 p, const DObject& o) {
+    V3 local = V3{o.c0.x * p.x + o.c1.x * p.y + o.c2.x * p.z + o.c3.x,
+                  o.c0.y * p.x + o.c1.y * p.y + o.c2.y * p.z + o.c3.y,
+                  o.c0.z * p.x + o.c1.z * p.y + o.c2.z * p.z + o.c3.z};
+    DMesh mesh = load_mesh(sc.meshes, o.info.x);
+    float d = mesh_distance(sc, local, mesh) * __uint_as_float(o.info.z);
+    if (d > 0.f) d *= .9999f;
+    return d;
+}
+
+struct Dist {
+    float best, voxel;
+    uint32_t closest;
+};
+
+// sdf.wgsl:42-60 — the cursor only moves forward (escape links point past
+// the subtree), so a walk visits at most 2N-1 nodes; a link that does not
+// advance is reported through the error word and ends the walk.
+template <bool NeedSpacing>
+__device__ __forceinline__ Dist scene_distance(const DevScene& sc, const irt_frame& f, V3 p, uint32_t hint) {
+    Dist r{1e20f, f.sdf[1], hint};
+    const uint32_t n = f.counts[3];
+    if (hint < n) {
+        DObject o = load_object(sc.objects, hint);
+        r.best = object_distance(sc, p, o);
+        if (NeedSpacing) r.voxel = __uint_as_float(o.info.w);
+    }
+    const uint32_t end = n * 2u - 1u;
+    uint32_t cursor = 0;
+    while (cursor < end) {
+        DNode node = load_node(sc.nodes, cursor);
+        V3 delta = vmax(vmax(xyz(node.lo) - p, p - xyz(node.hi)), V3{0.f, 0.f, 0.f});
+        V3 lb = delta * .9998f;
+        float b = wmax(r.best, 0.f);
+        if (dot(lb, lb) > b * b) {
+            uint32_t next = node.info.w;
+            if (next <= cursor) {
+                raise_error(sc.error, IRT_DEVERR_BVH_ESCAPE);
+                break;
+            }
+            cursor = next;
+            continue;
+        }
+        if (node.info.z == 1u) {
+            uint32_t oid = node.info.x;
+            if (oid != hint) {
+                DObject o = load_object(sc.objects, oid);
+                float d = object_distance(sc, p, o);
+                if (d < r.best) {
+                    r.best = d;
+                    r.voxel = NeedSpacing ? __uint_as_float(o.info.w) : f.sdf[1];
+                    r.closest = oid;
+                }
+            }
+        }
+        cursor++;
+    }
+    return r;
+}
+
+// sdf.wgsl:61-81 — soft-shadow visibility of `target` from surface point p.
+__device__ __forceinline__ float visibility(const DevScene& sc, const irt_frame& f, V3 p, V3 n, V3 target,
+                                            V3 end_normal) {
+    const float eps = f.sdf[1];
+    Dist clearance = scene_distance<true>(sc, f, p, 0xffffffffu);
+    float epsilon = wmax(eps, clearance.voxel * .65f);
+    uint32_t closest = clearance.closest;
+    V3 origin = p + n * epsilon;
+    V3 endpoint = target;
+    if (dot(end_normal, end_normal) > .5f) {
+        Dist e = scene_distance<true>(sc, f, target, 0xffffffffu);
+        endpoint = endpoint + end_normal * wmax(eps, e.voxel * .65f);
+    }
+    V3 delta = endpoint - origin;
+    float limit = length(delta) - eps;
+    if (limit <= 0.f) return 1.f;
+    V3 direction = normalize(delta);
+    float t = eps, result = 1.f, previous = 1e20f;
+    const uint32_t steps = to_u32(f.sdf[0]);
+    for (uint32_t i = 0; i < steps; i++) {
+        if (t >= limit) return wclamp(result, 0.f, 1.f);
+        Dist q = scene_distance<false>(sc, f, origin + direction * t, closest);
+        float h = q.best;
+        closest = q.closest;
+        if (h < eps) return 0.f;
+        float y = h * h / (2.f * previous);
+        float d = sqrtf(wmax(h * h - y * y, 0.f));
+        if (t > y) result = wmin(result, f.sdf[2] * d / (t - y));
+        if (result < .001f) return 0.f;
+        previous = h;
+        t += h;
+    }
+    return 0.f;
+}
+
+}  // namespace irtd

@@ -1,0 +1,204 @@
+// gbuffer.cu — CUDA G-buffer producer: one analytic primary ray per pixel
+// centre against the workload's boxes and spheres (stands in for the
+// gbuffer.wgsl raster; same outputs as irt_workload_gbuffer_cpu, in f32).
+#include <cuda_fp16.h>
+#include <cuda_runtime.h>
+
+#include <vector>
+
+#include "workload.h"
+
+namespace {
+
+using irt::GPrim;
+
+__device__ __forceinline__ void xf(const float* m, float x, float y, float z, float w, float o[4]) {
+#pragma unroll
+    for (int r = 0; r < 4; r++) o[r] = m[r] * x + m[4 + r] * y + m[8 + r] * z + m[12 + r] * w;
+}
+
+__device__ __forceinline__ uint16_t hbits(float v) { return __half_as_ushort(__float2half_rn(v)); }
+
+__device__ __forceinline__ uint32_t oct_snorm16(float x, float y, float z) {
+    float s = fabsf(x) + fabsf(y) + fabsf(z);
+    float u = x / s, v = y / s;
+    if (z < 0.f) {
+        float ou = (1.f - fabsf(v)) * (u >= 0.f ? 1.f : -1.f);
+        float ov = (1.f - fabsf(u)) * (v >= 0.f ? 1.f : -1.f);
+        u = ou;
+        v = ov;
+    }
+    int qu = __float2int_rn(fminf(fmaxf(u, -1.f), 1.f) * 32767.f);
+    int qv = __float2int_rn(fminf(fmaxf(v, -1.f), 1.f) * 32767.f);
+    return ((uint32_t)(uint16_t)(int16_t)qu) | ((uint32_t)(uint16_t)(int16_t)qv << 16);
+}
+
+__global__ void gbuffer_kernel(const __grid_constant__ irt_frame f, const GPrim* prims, uint32_t n_prims, int fmt,
+                               float* depth, void* normal, void* color, void* params, void* motion) {
+    uint32_t x = blockIdx.x * blockDim.x + threadIdx.x;
+    uint32_t y = blockIdx.y * blockDim.y + threadIdx.y;
+    uint32_t W = f.size[0], H = f.size[1];
+    if (x >= W || y >= H) return;
+    size_t i = (size_t)y * W + x;
+    float u = ((float)x + .5f) / (float)W, v = ((float)y + .5f) / (float)H;
+    float nx = u * 2.f - 1.f, ny = 1.f - v * 2.f;
+    float pn[4], pf[4];
+    xf(f.inv_vp.m, nx, ny, 0.f, 1.f, pn);
+    xf(f.inv_vp.m, nx, ny, 1.f, 1.f, pf);
+    float o[3] = {pn[0] / pn[3], pn[1] / pn[3], pn[2] / pn[3]};
+    float d[3] = {pf[0] / pf[3] - o[0], pf[1] / pf[3] - o[1], pf[2] / pf[3] - o[2]};
+    float best = 1.f;
+    int hit = -1;
+    float nl_best[3] = {0, 0, 0};
+    for (uint32_t k = 0; k < n_prims; k++) {
+        const GPrim& p = prims[k];
+        float lo4[4], ld4[4];
+        xf(p.inv_model, o[0], o[1], o[2], 1.f, lo4);
+        xf(p.inv_model, d[0], d[1], d[2], 0.f, ld4);
+        float t;
+        float nn[3] = {0, 0, 0};
+        bool h = false;
+        if (p.sphere) {
+            float r = p.lo[0];
+            float b = lo4[0] * ld4[0] + lo4[1] * ld4[1] + lo4[2] * ld4[2];
+            float a = ld4[0] * ld4[0] + ld4[1] * ld4[1] + ld4[2] * ld4[2];
+            float c = lo4[0] * lo4[0] + lo4[1] * lo4[1] + lo4[2] * lo4[2] - r * r;
+            float disc = b * b - a * c;
+            if (disc >= 0.f) {
+                t = (-b - sqrtf(disc)) / a;
+                if (t >= 0.f && t < best) {
+                    h = true;
+                    for (int q = 0; q < 3; q++) nn[q] = (lo4[q] + ld4[q] * t) / r;
+                }
+            }
+        } else {
+            float t0 = 0.f, t1 = best;
+            int axis = -1;
+            float sign = 0.f;
+            bool miss = false;
+            for (int a = 0; a < 3 && !miss; a++) {
+                float inv = 1.f / ld4[a];
+                float ta = (p.lo[a] - lo4[a]) * inv, tb = (p.hi[a] - lo4[a]) * inv;
+                float s = -1.f;
+                if (ta > tb) {
+                    float tmp = ta;
+                    ta = tb;
+                    tb = tmp;
+                    s = 1.f;
+                }
+                if (ta > t0) {
+                    t0 = ta;
+                    axis = a;
+                    sign = s;
+                }
+                t1 = fminf(t1, tb);
+                if (t0 > t1) miss = true;
+            }
+            if (!miss && axis >= 0 && t0 < best) {
+                h = true;
+                t = t0;
+                nn[axis] = sign;
+            }
+        }
+        if (h) {
+            best = t;
+            hit = (int)k;
+            nl_best[0] = nn[0];
+            nl_best[1] = nn[1];
+            nl_best[2] = nn[2];
+        }
+    }
+    float dep = 1.f, nrm[3] = {0, 0, 0}, col[3] = {0, 0, 0}, par[2] = {0, 0}, mot[2] = {0, 0};
+    if (hit >= 0) {
+        const GPrim& p = prims[hit];
+        float w[4];
+        xf(p.model, nl_best[0], nl_best[1], nl_best[2], 0.f, w);
+        float inv = 1.f / sqrtf(w[0] * w[0] + w[1] * w[1] + w[2] * w[2]);
+        nrm[0] = w[0] * inv;
+        nrm[1] = w[1] * inv;
+        nrm[2] = w[2] * inv;
+        float P[3] = {o[0] + d[0] * best, o[1] + d[1] * best, o[2] + d[2] * best};
+        float c[4], pc[4];
+        xf(f.vp.m, P[0], P[1], P[2], 1.f, c);
+        xf(f.previous_vp.m, P[0], P[1], P[2], 1.f, pc);
+        dep = fminf(c[2] / c[3], 0.99999994f);
+        col[0] = p.color[0];
+        col[1] = p.color[1];
+        col[2] = p.color[2];
+        par[0] = p.params[0];
+        par[1] = p.params[1];
+        mot[0] = (c[0] / c[3] - pc[0] / pc[3]) * .5f;
+        mot[1] = (c[1] / c[3] - pc[1] / pc[3]) * -.5f;
+    }
+    float alpha = hit >= 0 ? 1.f : 0.f;
+    depth[i] = dep;
+    if (fmt == IRT_GBUFFER_F32) {
+        ((float4*)normal)[i] = make_float4(nrm[0], nrm[1], nrm[2], alpha);
+        ((float4*)color)[i] = make_float4(col[0], col[1], col[2], alpha);
+        ((float2*)params)[i] = make_float2(par[0], par[1]);
+        ((float2*)motion)[i] = make_float2(mot[0], mot[1]);
+    } else if (fmt == IRT_GBUFFER_F16) {
+        ((uint2*)normal)[i] = make_uint2(hbits(nrm[0]) | ((uint32_t)hbits(nrm[1]) << 16), hbits(nrm[2]) | ((uint32_t)hbits(alpha) << 16));
+        ((uint2*)color)[i] = make_uint2(hbits(col[0]) | ((uint32_t)hbits(col[1]) << 16), hbits(col[2]) | ((uint32_t)hbits(alpha) << 16));
+        ((uint32_t*)params)[i] = hbits(par[0]) | ((uint32_t)hbits(par[1]) << 16);
+        ((uint32_t*)motion)[i] = hbits(mot[0]) | ((uint32_t)hbits(mot[1]) << 16);
+    } else {
+        ((uint32_t*)normal)[i] = hit >= 0 ? oct_snorm16(nrm[0], nrm[1], nrm[2]) : 0u;
+        auto q8 = [](float c) { return (uint32_t)__float2int_rn(fminf(fmaxf(c, 0.f), 1.f) * 255.f); };
+        ((uint32_t*)color)[i] = q8(col[0]) | (q8(col[1]) << 8) | (q8(col[2]) << 16) | (q8(alpha) << 24);
+        ((uint32_t*)params)[i] = hbits(par[0]) | ((uint32_t)hbits(par[1]) << 16);
+        ((uint32_t*)motion)[i] = hbits(mot[0]) | ((uint32_t)hbits(mot[1]) << 16);
+    }
+}
+
+}  // namespace
+
+extern "C" irt_status irt_gbuffer_render(irt_context* ctx, const irt_workload* wl_c, const irt_frame* f,
+                                         const irt_object* objects, int32_t format, float* depth, void* normal,
+                                         void* color, void* params, void* motion, void* stream) {
+    (void)objects;
+    if (!ctx || !wl_c || !f || !depth || !normal || !color || !params || !motion) return IRT_E_INVALID;
+    if (format < IRT_GBUFFER_F32 || format > IRT_GBUFFER_PACKED) return IRT_E_INVALID;
+    irt_workload* wl = const_cast<irt_workload*>(wl_c);
+    irt::Workload& w = wl->w;
+    int dev = 0;
+    cudaGetDevice(&dev);
+    // Flattened primitive table (static scenes: built once per device).
+    std::vector<GPrim> prims;
+    for (uint32_t oi = 0; oi < w.objs.size(); oi++) {
+        const irt::Obj& ob = w.objs[oi];
+        irt_mat4 model = irt::to_f32(ob.model), inv = irt::to_f32(ob.inv_model);
+        const irt_material& m = w.materials[ob.material];
+        for (const irt::Part& part : w.mesh_desc[ob.mesh].parts) {
+            GPrim g{};
+            for (int k = 0; k < 16; k++) {
+                g.inv_model[k] = inv.m[k];
+                g.model[k] = model.m[k];
+            }
+            for (int a = 0; a < 3; a++) {
+                g.lo[a] = part.sphere ? 0.f : (float)part.lo[a];
+                g.hi[a] = part.sphere ? 0.f : (float)part.hi[a];
+            }
+            if (part.sphere) g.lo[0] = (float)part.radius;
+            for (int k = 0; k < 3; k++) g.color[k] = m.color[k];
+            g.params[0] = fminf(fmaxf(m.params[0], .045f), 1.f);
+            g.params[1] = fminf(fmaxf(m.params[1], 0.f), 1.f);
+            g.object = oi;
+            g.sphere = part.sphere ? 1u : 0u;
+            prims.push_back(g);
+        }
+    }
+    if (!w.dev_prims || w.dev_prims_device != dev) {
+        if (w.dev_prims) cudaFree(w.dev_prims);
+        w.dev_prims = nullptr;
+        if (cudaMalloc(&w.dev_prims, prims.size() * sizeof(GPrim)) != cudaSuccess) return IRT_E_CUDA;
+        if (cudaMemcpy(w.dev_prims, prims.data(), prims.size() * sizeof(GPrim), cudaMemcpyHostToDevice) != cudaSuccess)
+            return IRT_E_CUDA;
+        w.dev_prims_device = dev;
+    }
+    dim3 block(32, 8);
+    dim3 grid((f->size[0] + 31) / 32, (f->size[1] + 7) / 8);
+    gbuffer_kernel<<<grid, block, 0, static_cast<cudaStream_t>(stream)>>>(
+        *f, static_cast<const GPrim*>(w.dev_prims), (uint32_t)prims.size(), format, depth, normal, color, params, motion);
+    return cudaGetLastError() == cudaSuccess ? IRT_OK : IRT_E_CUDA;
+}

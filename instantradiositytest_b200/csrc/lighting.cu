@@ -1,0 +1,390 @@
+// lighting.cu — the 8 lighting entry points of lighting.wgsl as sm_100a CUDA.
+//
+// Two schedules over the same per-pixel device functions:
+//   fused (default): reuse_kernel = candidates_direct + candidates_indirect +
+//     temporal_direct + temporal_indirect (writes reservoirs [1]);
+//     shade_kernel = spatial_direct + spatial_indirect + resolve_direct +
+//     resolve_indirect (writes reservoirs [2], direct and combined radiance).
+//   plain: one kernel per reference entry point (pass_kernel<Pass>).
+// Both write bit-identical results: the fused kernels call the same device
+// functions in the same order and keep intermediate reservoirs in registers
+// (f32 values identical to their stored form).
+// Threads: one per pixel, 32x8 blocks (warps span 32 consecutive pixels of a
+// row, so every own-pixel access is a coalesced 128-bit vector access).
+#include <cuda_runtime.h>
+
+#include "dev_sdf.cuh"
+#include "kernels.h"
+
+namespace irtd {
+
+template <class G>
+struct LightArgs {
+    G g;
+    DevScene sc;
+    const irt_vpl* cur;
+    const irt_vpl* prev;
+    const irt_vpl* arch;
+    const float* prev_depth;
+    const typename G::NormalT* prev_normal;
+    irt_reservoir* dres[3];
+    irt_reservoir* ires[3];
+    float4* direct_out;  // resolve_direct output (f32x4), may be null in fused mode
+    void* noisy_out;     // resolve_indirect output (radiance format)
+};
+
+template <class G>
+struct Px {
+    const irt_frame& f;
+    const LightArgs<G>& a;
+    uint32_t x, y;
+    size_t id;
+    __device__ __forceinline__ Px(const irt_frame& fr, const LightArgs<G>& ar, uint32_t px, uint32_t py)
+        : f(fr), a(ar), x(px), y(py), id((size_t)py * fr.size[0] + px) {}
+
+    __device__ __forceinline__ V3 camera() const { return V3{f.camera[0], f.camera[1], f.camera[2]}; }
+    __device__ __forceinline__ float uvx(uint32_t qx) const { return ((float)qx + .5f) / (float)f.size[0]; }
+    __device__ __forceinline__ float uvy(uint32_t qy) const { return ((float)qy + .5f) / (float)f.size[1]; }
+    __device__ __forceinline__ bool valid() const { return a.g.d(id) < 1.f; }
+    // lighting.wgsl:30-34
+    __device__ __forceinline__ Surface surface() const {
+        Surface s;
+        s.p = world(uvx(x), uvy(y), a.g.d(id), f.inv_vp);
+        s.n = normalize(a.g.n(id));
+        s.color = a.g.c(id);
+        float2 rm = a.g.pm(id);
+        s.rough = rm.x;
+        s.metal = rm.y;
+        return s;
+    }
+    // lighting.wgsl:36-40
+    __device__ __forceinline__ bool compatible(const Surface& s, uint32_t qx, uint32_t qy) const {
+        size_t q = (size_t)qy * f.size[0] + qx;
+        float d = a.g.d(q);
+        if (d >= 1.f) return false;
+        V3 p = world(uvx(qx), uvy(qy), d, f.inv_vp);
+        V3 n = normalize(a.g.n(q));
+        return dot(s.n, n) > f.temporal[2] && distance(s.p, p) < f.temporal[1] * wmax(distance(s.p, camera()), 1.f);
+    }
+    // lighting.wgsl:41-44
+    __device__ __forceinline__ void reproject(int32_t& qx, int32_t& qy) const {
+        float2 m = a.g.mv(id);
+        float u = uvx(x) - m.x, v = uvy(y) - m.y;
+        qx = to_i32(floorf(u * (float)f.size[0]));
+        qy = to_i32(floorf(v * (float)f.size[1]));
+    }
+    // lighting.wgsl:45-50
+    __device__ __forceinline__ bool history_valid(const Surface& s, int32_t qx, int32_t qy) const {
+        if (f.flags[0] == 0u || f.flags[1] != f.size[3] || qx < 0 || qy < 0 || qx >= (int32_t)f.size[0] ||
+            qy >= (int32_t)f.size[1])
+            return false;
+        size_t q = (size_t)qy * f.size[0] + (size_t)qx;
+        float d = __ldg(a.prev_depth + q);
+        if (d >= 1.f) return false;
+        V3 oldp = world(((float)qx + .5f) / (float)f.size[0], ((float)qy + .5f) / (float)f.size[1], d, f.previous_inv_vp);
+        V3 pn = G::decode_normal(__ldg(a.prev_normal + q));
+        return dot(s.n, pn) > f.temporal[2] && distance(s.p, oldp) < f.temporal[1] * wmax(distance(s.p, camera()), 1.f);
+    }
+    // lighting.wgsl:22-24
+    __device__ __forceinline__ bool vpl_sample_valid(const Res& r) const {
+        return r.generation == f.size[3] && r.target > 0.f && r.id < f.counts[1] &&
+               f.size[2] - r.source <= to_u32(f.rr[2]);
+    }
+    // lighting.wgsl:25-29
+    __device__ __forceinline__ DVpl selected_vpl(const Res& r) const {
+        if (r.source == f.size[2]) return load_vpl(a.cur, r.id);
+        if (r.source + 1u == f.size[2]) return load_vpl(a.prev, r.id);
+        uint32_t slots = to_u32(f.rr[2]) + 1u;
+        return load_vpl(a.arch, (size_t)(r.source % slots) * f.counts[1] + r.id);
+    }
+    // lighting.wgsl:86-89
+    __device__ __forceinline__ void neighbor(uint32_t& rng, int32_t& qx, int32_t& qy) const {
+        float angle = 2.f * kPI * rnd(rng);
+        float radius = sqrtf(rnd(rng)) * (float)f.restir[3];
+        qx = (int32_t)x + to_i32(rintf(cosf(angle) * radius));
+        qy = (int32_t)y + to_i32(rintf(sinf(angle) * radius));
+    }
+
+    // ---------------------------------------------------------------- passes
+    // lighting.wgsl:52-58
+    __device__ __forceinline__ Res candidates_direct(bool ok, const Surface& s) const {
+        Res r = res_empty(f);
+        uint32_t rng = seed((uint32_t)id, 11u, f.size[2]);
+        if (ok && f.counts[0] > 0u) {
+            float pdf = 1.f / (float)f.counts[0];
+            for (uint32_t i = 0; i < f.restir[0]; i++) {
+                uint32_t lid = min(to_u32(rnd(rng) * (float)f.counts[0]), f.counts[0] - 1u);
+                float target = luminance(direct(s, load_light(a.sc.lights, lid), camera()));
+                res_add(r, lid, f.size[2], target, pdf, target / pdf, 1u, 0u, rng);
+            }
+        }
+        return r;
+    }
+    // lighting.wgsl:59-65
+    __device__ __forceinline__ Res candidates_indirect(bool ok, const Surface& s) const {
+        Res r = res_empty(f);
+        uint32_t rng = seed((uint32_t)id, 13u, f.size[2]);
+        if (ok) {
+            float pdf = 1.f / (float)f.counts[1];
+            for (uint32_t i = 0; i < f.restir[1]; i++) {
+                uint32_t vid = min(to_u32(rnd(rng) * (float)f.counts[1]), f.counts[1] - 1u);
+                float target = luminance(indirect(s, load_vpl(a.cur, vid), camera()));
+                res_add(r, vid, f.size[2], target, pdf, target / pdf, 1u, 0u, rng);
+            }
+        }
+        return r;
+    }
+    // lighting.wgsl:66-74 (hv = valid && history_valid)
+    __device__ __forceinline__ void temporal_direct(Res& r, bool hv, const Surface& s, int32_t qx, int32_t qy) const {
+        uint32_t rng = seed((uint32_t)id, 17u, f.size[2]);
+        if (!hv) return;
+        Res previous = cap(res_load(a.dres[2], (size_t)qy * f.size[0] + (size_t)qx), to_u32(f.rr[2]) * f.restir[0]);
+        if (previous.generation == f.size[3] && previous.target > 0.f && previous.id < f.counts[0] &&
+            previous.age < to_u32(f.rr[2])) {
+            float target = luminance(direct(s, load_light(a.sc.lights, previous.id), camera()));
+            res_add(r, previous.id, previous.source, target, previous.pdf,
+                    target * normalization(previous) * (float)previous.count, previous.count, previous.age + 1u, rng);
+        }
+    }
+    // lighting.wgsl:75-85
+    __device__ __forceinline__ void temporal_indirect(Res& r, bool hv, const Surface& s, int32_t qx, int32_t qy) const {
+        uint32_t rng = seed((uint32_t)id, 19u, f.size[2]);
+        if (!hv) return;
+        Res previous = cap(res_load(a.ires[2], (size_t)qy * f.size[0] + (size_t)qx), to_u32(f.rr[2]) * f.restir[1]);
+        if (vpl_sample_valid(previous)) {
+            float target = luminance(indirect(s, selected_vpl(previous), camera()));
+            res_add(r, previous.id, previous.source, target, previous.pdf,
+                    target * normalization(previous) * (float)previous.count, previous.count, previous.age + 1u, rng);
+        }
+    }
+    // lighting.wgsl:90-97 / 98-105 — reservoir `r` is the pixel's own [1].
+    template <int Dom>
+    __device__ __forceinline__ Res spatial(Res r, bool ok, const Surface& s) const {
+        uint32_t rng = seed((uint32_t)id, Dom == 0 ? 23u : 29u, f.size[2]);
+        const irt_reservoir* in = Dom == 0 ? a.dres[1] : a.ires[1];
+        if (ok) {
+            for (uint32_t i = 0; i < f.restir[2]; i++) {
+                int32_t qx, qy;
+                neighbor(rng, qx, qy);
+                if (qx < 0 || qy < 0 || qx >= (int32_t)f.size[0] || qy >= (int32_t)f.size[1]) continue;
+                if (!compatible(s, (uint32_t)qx, (uint32_t)qy)) continue;
+                Res previous = res_load(in, (size_t)qy * f.size[0] + (size_t)qx);
+                if (Dom == 0) {
+                    if (previous.target > 0.f) {
+                        float target = luminance(direct(s, load_light(a.sc.lights, previous.id), camera()));
+                        res_add(r, previous.id, previous.source, target, previous.pdf,
+                                target * normalization(previous) * (float)previous.count, previous.count, previous.age,
+                                rng);
+                    }
+                } else if (vpl_sample_valid(previous)) {
+                    float target = luminance(indirect(s, selected_vpl(previous), camera()));
+                    res_add(r, previous.id, previous.source, target, previous.pdf,
+                            target * normalization(previous) * (float)previous.count, previous.count, previous.age, rng);
+                }
+            }
+        }
+        return cap(r, to_u32(f.rr[2]) * f.restir[Dom] * 8u);
+    }
+    // lighting.wgsl:106-122
+    __device__ __forceinline__ V3 resolve_direct(bool ok, const Surface& s, const Res& d) const {
+        V3 result = V3{0.f, 0.f, 0.f};
+        if (ok) {
+            uint32_t dbg = f.flags[2];
+            if (d.target > 0.f && dbg != 2u && dbg < 3u) {
+                DLight l = load_light(a.sc.lights, d.id);
+                V3 value = direct(s, l, camera());
+                if (luminance(value) > 0.f) {
+                    float vis = visibility(a.sc, f, s.p, s.n, xyz(l.ps), V3{0.f, 0.f, 0.f});
+                    float k = normalization(d);
+                    result = result + V3{value.x * k * vis, value.y * k * vis, value.z * k * vis};
+                }
+            }
+            if (dbg == 3u) result = s.color;
+            if (dbg == 4u) result = V3{s.n.x * .5f + .5f, s.n.y * .5f + .5f, s.n.z * .5f + .5f};
+            if (dbg == 5u) {
+                float2 m = a.g.mv(id);
+                result = V3{wclamp(.5f + m.x * 50.f, 0.f, 1.f), wclamp(.5f + m.y * 50.f, 0.f, 1.f), .5f};
+            }
+        }
+        return result;
+    }
+    // lighting.wgsl:123-134 (before the 65000 clamp)
+    __device__ __forceinline__ V3 resolve_indirect(bool ok, const Surface& s, const Res& v, V3 result) const {
+        uint32_t dbg = f.flags[2];
+        if (ok && dbg != 1u && dbg < 3u) {
+            if (vpl_sample_valid(v)) {
+                DVpl smp = selected_vpl(v);
+                V3 value = indirect(s, smp, camera());
+                if (luminance(value) > 0.f) {
+                    float vis = visibility(a.sc, f, s.p, s.n, xyz(smp.pos), xyz(smp.nrm));
+                    float k = normalization(v);
+                    result = result + V3{value.x * k * vis, value.y * k * vis, value.z * k * vis};
+                }
+            }
+        }
+        return result;
+    }
+};
+
+template <class R>
+__device__ __forceinline__ void store_noisy(void* out, size_t i, V3 r) {
+    R::store(reinterpret_cast<typename R::T*>(out), i, make_float4(wmin(r.x, 65000.f), wmin(r.y, 65000.f), wmin(r.z, 65000.f), 1.f));
+}
+
+// ---------------------------------------------------------------- fused kernels
+template <class G>
+__global__ void __launch_bounds__(256) reuse_kernel(const __grid_constant__ irt_frame f, const __grid_constant__ LightArgs<G> a,
+                                                    int keep_candidates) {
+    uint32_t x = blockIdx.x * blockDim.x + threadIdx.x;
+    uint32_t y = blockIdx.y * blockDim.y + threadIdx.y;
+    if (x >= f.size[0] || y >= f.size[1]) return;
+    Px<G> px(f, a, x, y);
+    bool ok = px.valid();
+    Surface s;
+    if (ok) s = px.surface();
+    Res rd = px.candidates_direct(ok, s);
+    Res ri = px.candidates_indirect(ok, s);
+    if (keep_candidates) {
+        res_store(a.dres[0], px.id, rd);
+        res_store(a.ires[0], px.id, ri);
+    }
+    int32_t qx, qy;
+    px.reproject(qx, qy);
+    bool hv = ok && px.history_valid(s, qx, qy);
+    px.temporal_direct(rd, hv, s, qx, qy);
+    px.temporal_indirect(ri, hv, s, qx, qy);
+    res_store(a.dres[1], px.id, rd);
+    res_store(a.ires[1], px.id, ri);
+}
+
+template <class G, class R>
+__global__ void __launch_bounds__(256) shade_kernel(const __grid_constant__ irt_frame f, const __grid_constant__ LightArgs<G> a) {
+    uint32_t x = blockIdx.x * blockDim.x + threadIdx.x;
+    uint32_t y = blockIdx.y * blockDim.y + threadIdx.y;
+    if (x >= f.size[0] || y >= f.size[1]) return;
+    Px<G> px(f, a, x, y);
+    bool ok = px.valid();
+    Surface s;
+    if (ok) s = px.surface();
+    Res rd = px.template spatial<0>(res_load(a.dres[1], px.id), ok, s);
+    res_store(a.dres[2], px.id, rd);
+    Res ri = px.template spatial<1>(res_load(a.ires[1], px.id), ok, s);
+    res_store(a.ires[2], px.id, ri);
+    V3 direct_result = px.resolve_direct(ok, s, rd);
+    if (a.direct_out) a.direct_out[px.id] = make_float4(direct_result.x, direct_result.y, direct_result.z, 1.f);
+    V3 total = px.resolve_indirect(ok, s, ri, direct_result);
+    store_noisy<R>(a.noisy_out, px.id, total);
+}
+
+// ---------------------------------------------------------------- plain kernels
+template <class G, class R, int Pass>
+__global__ void __launch_bounds__(256) pass_kernel(const __grid_constant__ irt_frame f, const __grid_constant__ LightArgs<G> a) {
+    uint32_t x = blockIdx.x * blockDim.x + threadIdx.x;
+    uint32_t y = blockIdx.y * blockDim.y + threadIdx.y;
+    if (x >= f.size[0] || y >= f.size[1]) return;
+    Px<G> px(f, a, x, y);
+    bool ok = px.valid();
+    Surface s;
+    if (ok) s = px.surface();
+    if (Pass == 0) {
+        res_store(a.dres[0], px.id, px.candidates_direct(ok, s));
+    } else if (Pass == 1) {
+        res_store(a.ires[0], px.id, px.candidates_indirect(ok, s));
+    } else if (Pass == 2 || Pass == 3) {
+        int32_t qx, qy;
+        px.reproject(qx, qy);
+        bool hv = ok && px.history_valid(s, qx, qy);
+        if (Pass == 2) {
+            Res r = res_load(a.dres[0], px.id);
+            px.temporal_direct(r, hv, s, qx, qy);
+            res_store(a.dres[1], px.id, r);
+        } else {
+            Res r = res_load(a.ires[0], px.id);
+            px.temporal_indirect(r, hv, s, qx, qy);
+            res_store(a.ires[1], px.id, r);
+        }
+    } else if (Pass == 4) {
+        res_store(a.dres[2], px.id, px.template spatial<0>(res_load(a.dres[1], px.id), ok, s));
+    } else if (Pass == 5) {
+        res_store(a.ires[2], px.id, px.template spatial<1>(res_load(a.ires[1], px.id), ok, s));
+    } else if (Pass == 6) {
+        V3 r = px.resolve_direct(ok, s, res_load(a.dres[2], px.id));
+        a.direct_out[px.id] = make_float4(r.x, r.y, r.z, 1.f);
+    } else {
+        float4 d = a.direct_out[px.id];
+        V3 total = px.resolve_indirect(ok, s, res_load(a.ires[2], px.id), V3{d.x, d.y, d.z});
+        store_noisy<R>(a.noisy_out, px.id, total);
+    }
+}
+
+// ---------------------------------------------------------------- host launchers
+template <class G>
+static LightArgs<G> make_args(const LightingLaunch& L) {
+    LightArgs<G> a;
+    a.g.depth = L.gbuffer.depth;
+    a.g.normal = reinterpret_cast<decltype(a.g.normal)>(L.gbuffer.normal);
+    a.g.color = reinterpret_cast<decltype(a.g.color)>(L.gbuffer.color);
+    a.g.params = reinterpret_cast<decltype(a.g.params)>(L.gbuffer.params);
+    a.g.motion = reinterpret_cast<decltype(a.g.motion)>(L.gbuffer.motion);
+    a.sc.objects = L.objects;
+    a.sc.meshes = L.meshes;
+    a.sc.nodes = L.nodes;
+    a.sc.lights = L.lights;
+    a.sc.atlas = L.atlas;
+    a.sc.sdf_f16 = L.sdf_f16;
+    a.sc.error = L.error;
+    a.cur = L.cur_vpls;
+    a.prev = L.prev_vpls;
+    a.arch = L.archive;
+    a.prev_depth = L.prev_depth;
+    a.prev_normal = reinterpret_cast<const typename G::NormalT*>(L.prev_normal);
+    for (int k = 0; k < 3; k++) {
+        a.dres[k] = L.dres[k];
+        a.ires[k] = L.ires[k];
+    }
+    a.direct_out = L.direct_out;
+    a.noisy_out = L.noisy_out;
+    return a;
+}
+
+template <class G, class R>
+static cudaError_t launch_typed(const LightingLaunch& L, int stage, cudaStream_t st) {
+    LightArgs<G> a = make_args<G>(L);
+    const irt_frame& f = *L.frame;
+    dim3 block(32, 8);
+    dim3 grid((f.size[0] + 31) / 32, (f.size[1] + 7) / 8);
+    switch (stage) {
+    case kStageReuse: reuse_kernel<G><<<grid, block, 0, st>>>(f, a, L.keep_candidates); break;
+    case kStageShade: shade_kernel<G, R><<<grid, block, 0, st>>>(f, a); break;
+    case 0: pass_kernel<G, R, 0><<<grid, block, 0, st>>>(f, a); break;
+    case 1: pass_kernel<G, R, 1><<<grid, block, 0, st>>>(f, a); break;
+    case 2: pass_kernel<G, R, 2><<<grid, block, 0, st>>>(f, a); break;
+    case 3: pass_kernel<G, R, 3><<<grid, block, 0, st>>>(f, a); break;
+    case 4: pass_kernel<G, R, 4><<<grid, block, 0, st>>>(f, a); break;
+    case 5: pass_kernel<G, R, 5><<<grid, block, 0, st>>>(f, a); break;
+    case 6: pass_kernel<G, R, 6><<<grid, block, 0, st>>>(f, a); break;
+    case 7: pass_kernel<G, R, 7><<<grid, block, 0, st>>>(f, a); break;
+    default: return cudaErrorInvalidValue;
+    }
+    return cudaGetLastError();
+}
+
+}  // namespace irtd
+
+cudaError_t irt_launch_lighting(const LightingLaunch& L, int stage, cudaStream_t st) {
+    using namespace irtd;
+    if (L.radiance_f16) {
+        switch (L.gbuffer.format) {
+        case IRT_GBUFFER_F32: return launch_typed<GbF32, RadF16>(L, stage, st);
+        case IRT_GBUFFER_F16: return launch_typed<GbF16, RadF16>(L, stage, st);
+        case IRT_GBUFFER_PACKED: return launch_typed<GbPacked, RadF16>(L, stage, st);
+        }
+    } else {
+        switch (L.gbuffer.format) {
+        case IRT_GBUFFER_F32: return launch_typed<GbF32, RadF32>(L, stage, st);
+        case IRT_GBUFFER_F16: return launch_typed<GbF16, RadF32>(L, stage, st);
+        case IRT_GBUFFER_PACKED: return launch_typed<GbPacked, RadF32>(L, stage, st);
+        }
+    }
+    return cudaErrorInvalidValue;
+}

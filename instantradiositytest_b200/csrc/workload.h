@@ -1,0 +1,82 @@
+// workload.h — seeded procedural room workloads (host side).
+#pragma once
+#include <cstdint>
+#include <vector>
+
+#include "../../include/irt.h"
+#include "host_math.h"
+
+namespace irt {
+
+struct Part {  // one analytic solid of a mesh, in mesh-local space
+    bool sphere = false;
+    double radius = 0;
+    double lo[3] = {0, 0, 0}, hi[3] = {0, 0, 0};
+};
+
+struct MeshDesc {
+    std::vector<Part> parts;
+    std::vector<irt_vertex> vertices;
+    std::vector<uint32_t> indices;
+    float sdf_lo[3], sdf_hi[3];
+};
+
+struct Obj {
+    uint32_t mesh, material;
+    M4 model, inv_model;
+};
+
+struct Workload {
+    irt_workload_spec spec{};
+    std::vector<MeshDesc> mesh_desc;
+    std::vector<Obj> objs;
+    std::vector<irt_material> materials;
+    std::vector<irt_light> lights;
+    std::vector<irt_mesh> meshes;
+    std::vector<std::vector<float>> mesh_samples;
+    std::vector<float> atlas32;
+    std::vector<uint16_t> atlas16;
+    uint32_t atlas_dims[3] = {0, 0, 0}, atlas_grid[3] = {0, 0, 0};
+    uint32_t path_frames = 64;
+    double angle0 = 0;
+    // Device copy of the analytic primitive table for the CUDA G-buffer
+    // producer (lazily created, owned here).
+    void* dev_prims = nullptr;
+    int dev_prims_device = -1;
+
+    bool build();
+    void camera_at(uint32_t frame, double eye[3], double target[3]) const;
+    M4 view_projection(uint32_t frame) const;
+    void frame_data(uint32_t index, uint32_t debug, irt_frame* f, irt_object* objects, irt_node* nodes,
+                    irt_light* lights) const;
+    void settings(irt_settings* s) const;
+    bool intersect_object(uint32_t oi, const double o[3], const double d[3], double tmin, double tmax, double& t,
+                          double n[3]) const;
+    bool cast(const double o[3], const double d[3], double tmin, double tmax, double& t, double n[3],
+              uint32_t& object) const;
+};
+
+uint16_t f16_bits_rne(float f);
+float f16_bits_to_f32(uint16_t h);
+uint16_t f16_bits_round_down(float v);
+
+// Octahedral unit-vector encoding to two snorm16 (Cigolle et al. 2014).
+uint32_t oct_encode_snorm16(float x, float y, float z);
+// rgba8 unorm packing with round-to-nearest.
+uint32_t pack_unorm8x4(float r, float g, float b, float a);
+
+// Flattened primitive record used by the CUDA G-buffer producer.
+struct GPrim {
+    float inv_model[16];
+    float model[16];
+    float lo[4], hi[4];  // box bounds (local) or radius in lo[0] for spheres
+    float color[4];
+    float params[4];     // roughness, metal after material clamping
+    uint32_t object, sphere, pad0, pad1;
+};
+
+}  // namespace irt
+
+struct irt_workload {
+    irt::Workload w;
+};

@@ -1,0 +1,118 @@
+"""Shared GPU-test harness: runs the CUDA path and the CPU oracle on the same
+inputs, frame by frame, and measures the agreement the parity bar asks for.
+
+Agreement metrics
+  * selection: fraction of pixels whose reservoir (id, source, count, age)
+    is bit-identical — the bar is >= 99.9 %;
+  * radiance: mean relative error sum|a - b| / sum|b| over all pixels and
+    channels (relative L1) — the bar is <= 1e-3.
+"""
+from __future__ import annotations
+
+import numpy as np
+import torch
+
+from instantradiositytest_b200 import _lib as L
+from instantradiositytest_b200.runtime import FrameDriver
+from instantradiositytest_b200.workload import Workload, gbuffer_as_f32
+from oracle import Oracle, OracleScene
+from oracle import binding as ob
+
+SELECT_BAR = 0.999
+RADIANCE_BAR = 1e-3
+
+
+def rel_l1(a, b):
+    a = np.asarray(a, np.float64)
+    b = np.asarray(b, np.float64)
+    den = np.abs(b).sum()
+    return float(np.abs(a - b).sum() / den) if den > 0 else float(np.abs(a - b).sum())
+
+
+def selection_match(a, b):
+    keys = ("id", "source", "count", "age")
+    same = np.ones(len(a), bool)
+    for k in keys:
+        same &= a[k] == b[k]
+    return float(same.mean())
+
+
+def sync_history(orc: Oracle, drv: FrameDriver, prev_index: int):
+    """Copy the GPU session's history (the state the next frame reads) into
+    the oracle so a frame can be compared without accumulated drift."""
+    s = drv.session
+    for dom, key in ((0, "d"), (1, "i")):
+        orc.reservoirs(key, 2, L.RESERVOIR_DTYPE)[:] = s.reservoirs_host(dom, 2)
+    arch_ptr, arch_bytes = s.buffer_ptr(L.BUF_VPL_ARCHIVE)
+    orc.buffer(ob.ARCHIVE, np.uint8)[:] = s.buffer(L.BUF_VPL_ARCHIVE, torch.uint8).cpu().numpy()
+    orc.buffer(ob.PREV_DEPTH)[:] = s.buffer(L.BUF_PREV_DEPTH).cpu().numpy()
+    pn = s.buffer(L.BUF_PREV_NORMAL, torch.uint8).cpu().numpy()
+    if drv.fmt == L.GBUFFER_F32:
+        pn = pn.view(np.float32)
+    elif drv.fmt == L.GBUFFER_F16:
+        pn = pn.view(np.float16).astype(np.float32)
+    else:
+        from instantradiositytest_b200.workload import oct_decode_f32
+
+        n3 = oct_decode_f32(pn.view(np.uint32))
+        pn = np.concatenate([n3, np.zeros(n3.shape[:-1] + (1,), np.float32)], -1).reshape(-1)
+    orc.buffer(ob.PREV_NORMAL)[:] = pn.reshape(-1)
+    k = prev_index % 2
+    orc.buffer(ob.MOMENTS[k])[:] = s.image_host(L.BUF_MOMENTS).reshape(-1)
+    orc.buffer(ob.FEEDBACK[k])[:] = s.image_host(L.BUF_FEEDBACK).reshape(-1)
+
+
+class Lockstep:
+    def __init__(self, wl: Workload, gbuffer_format=L.GBUFFER_F32, radiance_format=L.RADIANCE_F32, fused=True,
+                 precision=0):
+        self.wl = wl
+        self.drv = FrameDriver(wl, gbuffer_format=gbuffer_format, radiance_format=radiance_format, fused=fused,
+                               keep_candidates=True)
+        self.orc = Oracle(wl.width, wl.height, wl.settings.vpl_count, wl.settings.restir_max_history, precision,
+                          radiance_format == L.RADIANCE_F16)
+        self.fmt = gbuffer_format
+        self.prev_vpls = None
+
+    def frame(self, index: int, sync=True, debug=0):
+        inputs = self.drv.inputs(index, debug)
+        f, obj, nodes, lights, planes, vpls = inputs
+        if sync and index > 0:
+            sync_history(self.orc, self.drv, index - 1)
+        self.drv.step(index, debug, inputs=inputs)
+        torch.cuda.synchronize()
+        prev = self.prev_vpls if self.prev_vpls is not None else np.zeros_like(vpls)
+        sc = OracleScene(obj, self.wl.meshes, nodes, lights, atlas_f32(self.wl))
+        self.orc.frame(f, sc, gbuffer_as_f32(planes, self.fmt), vpls, prev, self.wl.settings.svgf_iterations)
+        self.prev_vpls = vpls
+        return self.compare(index)
+
+    def compare(self, index: int):
+        s, o = self.drv.session, self.orc
+        out = {}
+        for dom, key in ((0, "d"), (1, "i")):
+            for k in (0, 1, 2):
+                out[f"select_{key}{k}"] = selection_match(s.reservoirs_host(dom, k),
+                                                          o.reservoirs(key, k, L.RESERVOIR_DTYPE))
+        out["direct"] = rel_l1(s.image_host(L.BUF_DIRECT)[..., :3], o.image(ob.DIRECT)[..., :3])
+        out["noisy"] = rel_l1(s.image_host(L.BUF_NOISY)[..., :3], o.image(ob.LIGHTING)[..., :3])
+        out["filtered"] = rel_l1(s.image_host(L.BUF_FILTERED)[..., :3], o.image(ob.HISTORIES[index % 2])[..., :3])
+        out["moments"] = rel_l1(s.image_host(L.BUF_MOMENTS)[..., :3], o.image(ob.MOMENTS[index % 2])[..., :3])
+        return out
+
+    def close(self):
+        self.drv.close()
+        self.orc.close()
+
+
+def atlas_f32(wl: Workload) -> np.ndarray:
+    """The SDF texels the kernels see, dequantised (f16 x per-mesh scale)."""
+    if wl.sdf_format == L.SDF_F32:
+        return wl.atlas
+    a = wl.atlas.view(np.float16).astype(np.float32)
+    out = np.empty_like(a)
+    # each mesh tile carries its own scale in irt_mesh.lo[3]
+    out[:] = a
+    for m in wl.meshes:
+        x, y, z, r = (int(v) for v in m["field"])
+        out[z:z + r, y:y + r, x:x + r] = a[z:z + r, y:y + r, x:x + r] * np.float32(m["lo"][3])
+    return out

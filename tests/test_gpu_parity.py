@@ -1,0 +1,121 @@
+"""Parity of the CUDA lighting path (through the C-ABI) with the CPU oracle.
+
+Per frame the oracle starts from the GPU's history (reservoirs [2], VPL
+archive, SVGF moments/feedback, previous depth/normal), so every frame is an
+independent parity case of all 11 reference passes; a free-running run then
+checks that the accumulated images stay within the radiance bar.
+"""
+import numpy as np
+import pytest
+import torch
+
+from instantradiositytest_b200 import _lib as L
+from instantradiositytest_b200.runtime import FrameDriver
+from instantradiositytest_b200.workload import Workload
+
+from gpu_harness import RADIANCE_BAR, SELECT_BAR, Lockstep, rel_l1
+
+pytestmark = pytest.mark.gpu
+
+
+def summarize(rows):
+    keys = rows[0].keys()
+    return {k: (min(r[k] for r in rows) if k.startswith("select") else max(r[k] for r in rows)) for k in keys}
+
+
+def check(stats, label):
+    for k, v in stats.items():
+        if k.startswith("select"):
+            assert v >= SELECT_BAR, f"{label}: {k} = {v}"
+        else:
+            assert v <= RADIANCE_BAR, f"{label}: {k} = {v}"
+
+
+@pytest.mark.parametrize("fused", [True, False])
+def test_small_room_lockstep_parity(cuda, fused):
+    """256x160 room of 12 meshes, 16 frames, f32 G-buffer and radiance."""
+    wl = Workload(0)
+    ls = Lockstep(wl, fused=fused)
+    rows = [ls.frame(i) for i in range(16)]
+    ls.close()
+    stats = summarize(rows)
+    print("lockstep", "fused" if fused else "plain", stats)
+    check(stats, "lockstep")
+
+
+def test_reference_formats_lockstep_parity(cuda):
+    """The reference's own storage formats: Rgba16Float G-buffer, noisy and
+    SVGF radiance, Rgba32Float moments."""
+    wl = Workload(0, width=160, height=100)
+    ls = Lockstep(wl, gbuffer_format=L.GBUFFER_F16, radiance_format=L.RADIANCE_F16)
+    rows = [ls.frame(i) for i in range(10)]
+    ls.close()
+    stats = summarize(rows)
+    print("f16 formats", stats)
+    check(stats, "f16")
+
+
+def test_free_running_images_stay_within_bar(cuda):
+    wl = Workload(0)
+    ls = Lockstep(wl)
+    for i in range(16):
+        r = ls.frame(i, sync=False)
+    ls.close()
+    print("free running, frame 15", r)
+    assert r["noisy"] <= 5 * RADIANCE_BAR  # drift allowance over 16 frames without re-sync
+    assert r["filtered"] <= 5 * RADIANCE_BAR
+
+
+def test_fused_and_plain_schedules_are_bit_identical(cuda):
+    wl = Workload(0, width=128, height=96)
+    a = FrameDriver(wl, fused=True, keep_candidates=True)
+    b = FrameDriver(wl, fused=False)
+    for i in range(6):
+        inputs = a.inputs(i)
+        a.step(i, inputs=inputs)
+        b.step(i, inputs=inputs)
+    torch.cuda.synchronize()
+    for dom in (0, 1):
+        for k in (0, 1, 2):
+            assert np.array_equal(a.session.reservoirs_host(dom, k).view(np.uint8),
+                                  b.session.reservoirs_host(dom, k).view(np.uint8)), (dom, k)
+    for which in (L.BUF_DIRECT, L.BUF_NOISY, L.BUF_FILTERED, L.BUF_MOMENTS, L.BUF_FEEDBACK):
+        assert np.array_equal(a.session.image_host(which), b.session.image_host(which)), which
+    a.close()
+    b.close()
+
+
+def test_two_runs_are_bit_identical(cuda):
+    # tools/verify.py:61-67 demands identical captures at tolerance 0.
+    wl = Workload(0, width=96, height=64)
+    outs = []
+    for _ in range(2):
+        d = FrameDriver(wl)
+        for i in range(5):
+            d.step(i)
+        torch.cuda.synchronize()
+        outs.append((d.session.image_host(L.BUF_FILTERED), d.session.reservoirs_host(1, 2).view(np.uint8)))
+        d.close()
+    assert np.array_equal(outs[0][0], outs[1][0])
+    assert np.array_equal(outs[0][1], outs[1][1])
+
+
+def test_outputs_finite_capped_and_error_word_clear(cuda):
+    wl = Workload(0)
+    d = FrameDriver(wl)
+    for i in range(8):
+        d.step(i)
+    torch.cuda.synchronize()
+    assert d.session.check() == L.IRT_OK
+    for which in (L.BUF_DIRECT, L.BUF_NOISY, L.BUF_FILTERED):
+        img = d.session.image_host(which)
+        assert np.all(np.isfinite(img)) and np.all(img[..., :3] >= 0)
+    s = d.settings if hasattr(d, "settings") else wl.settings
+    for dom, cand in ((0, s.restir_direct_candidates), (1, s.restir_vpl_candidates)):
+        r = d.session.reservoirs_host(dom, 2)
+        assert r["count"].max() <= s.restir_max_history * cand * 8
+        assert r["count"].max() >= s.restir_max_history * cand  # temporal reuse retained
+        assert r["age"].max() <= s.restir_max_history
+    m = d.session.image_host(L.BUF_MOMENTS)
+    assert m[..., 2].max() >= 6  # SVGF history accumulates on the static room
+    d.close()
