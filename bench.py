@@ -37,21 +37,30 @@ sys.path.insert(0, ROOT)
 # Algorithmic bytes per pixel and kernel for the f32 G-buffer / f32 radiance
 # schedule (every surface counted once per kernel that touches it; neighbour
 # taps are cache traffic, not HBM):
-#   reuse  = G-buffer 44 (depth 4, normal 12, colour 12, params 8, motion 8)
-#            + previous depth/normal 16 + history reservoirs D/I 64
-#            + reservoirs [1] D/I written 64                          = 188
-#   shade  = G-buffer 36 (no motion) + reservoirs [1] 64 + [2] written 64
-#            + direct f32x4 16 + noisy f32x4 16                       = 196
+#   reuse   = G-buffer 44 (depth 4, normal 12, colour 12, params 8, motion 8)
+#             + previous depth/normal 16 + history reservoirs D/I 64
+#             + reservoirs [1] D/I written 64                         = 188
+#   spatial = G-buffer 36 (no motion) + reservoirs [1] 64 + [2] written 64
+#             + contributions 32 + 2 ray records 128 written          = 324
+#   march   = 2 ray records 128 read + 2 visibilities 8 written       = 136
+#   combine = contributions 32 + visibilities 8 + direct 16 + noisy 16 = 72
 #   svgf_temporal = noisy 16 + G-buffer 44 + feedback 16 + moments 16
-#            + previous depth/normal 16 + temporal 16 + moments 16    = 140
+#             + previous depth/normal 16 + temporal 16 + moments 16   = 140
 #   svgf_variance = temporal 16 + moments 16 + G-buffer guides 36
-#            + output 16                                              =  84
-#   atrous = input 16 + guides 36 + output 16                         =  68 (x4)
+#             + output 16                                             =  84
+#   atrous  = input 16 + guides 36 + output 16                        =  68 (x4)
 #   history copy = depth+normal read 20 + write 20                    =  40
-ALG_BYTES = {"reuse": 188, "shade": 196, "svgf_temporal": 140, "svgf_variance": 84, "atrous": 4 * 68,
-             "history": 40}
-STAGES = ["archive", "reuse", "shade", "svgf_temporal", "svgf_variance", "atrous", "history"]
-KERNELS_PER_FRAME_FUSED = 2 + 2 + 4  # reuse, shade, svgf temporal, variance, 4 a-trous
+ALG_BYTES = {"reuse": 188, "spatial": 324, "march": 136, "combine": 72, "svgf_temporal": 140, "svgf_variance": 84,
+             "atrous": 4 * 68, "history": 40}
+STAGES = ["archive", "reuse", "spatial", "march", "combine", "svgf_temporal", "svgf_variance", "atrous", "history"]
+KERNELS = ["reuse", "spatial", "march", "combine", "svgf_temporal", "svgf_variance", "atrous"]
+KERNELS_PER_FRAME = 4 + 2 + 4  # reuse, spatial, march, combine, svgf temporal, variance, 4 a-trous
+# Counted FP32 work of the march per oracle work counter (flops): BVH node
+# visit (box test), certified-box distance, field distance (transform,
+# trilinear, bounds), march step (penumbra update).
+FLOPS_PER = {"nodes": 15, "box_queries": 50, "field_queries": 90, "march_steps": 15}
+# Nominal B200 FP32 SIMT peak: 148 SMs x 128 lanes x 2 flops x 1.965 GHz.
+FP32_PEAK_TFLOPS = 148 * 128 * 2 * 1.965e9 / 1e12
 
 
 def parse():
@@ -63,7 +72,8 @@ def parse():
     ap.add_argument("--config", type=int, default=1)
     ap.add_argument("--width", type=int, default=0)
     ap.add_argument("--height", type=int, default=0)
-    ap.add_argument("--plain", action="store_true", help="one kernel per reference entry point")
+    ap.add_argument("--schedule", type=int, default=1, choices=[0, 1, 2],
+                    help="1 ray-queue march (default), 2 fused with the march inline, 0 one kernel per entry point")
     ap.add_argument("--no-e2e", action="store_true")
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--cpu-seconds", type=float, default=15.0, help="CPU work budget of the cpu_baseline sample")
@@ -163,10 +173,11 @@ def measured_peak():
         return 6650.0, "fallback"
 
 
-def ncu_traffic():
-    """dram bytes per launch of the shade kernel from the committed ncu
-    summary (profiles/shade_kernel_1920x1200.md, line `dram_bytes_per_launch:`)."""
-    path = os.path.join(ROOT, "profiles", "shade_kernel_1920x1200.md")
+def ncu_traffic(kernel):
+    """DRAM bytes (read + write) per launch of `kernel` at 1920x1200 from the
+    committed ncu summary profiles/<kernel>_kernel_1920x1200.md (its line
+    `dram_bytes_per_launch: N`), or None when no capture is committed."""
+    path = os.path.join(ROOT, "profiles", f"{kernel}_kernel_1920x1200.md")
     try:
         for line in open(path):
             if line.startswith("dram_bytes_per_launch:"):
@@ -220,10 +231,13 @@ def cpu_run(spec, steps, warmup, budget_s, threads=0):
     for i in range(warmup + 1, warmup + 1 + steps):
         total += run(i, rows)
     threads_used = orc.threads
+    counters = orc.counters()  # of the last frame's band
     orc.close()
     wl.close()
     px = rows * W * steps
+    per_px = {k: v / (rows * W) for k, v in counters.items()}
     return {"value": px / total / 1e6, "seconds": total, "rows": rows, "steps": steps, "threads": threads_used,
+            "counters_per_pixel": per_px,
             "sample": f"{rows} of {H} rows (centre band) x {W} columns, {steps} timed frames after "
                       f"{warmup + 1} warm-up frames, full SVGF + lighting on the band"}
 
@@ -278,8 +292,8 @@ def ours(args):
     n_frames = K + Wm
     ctx = Context(dev)
     scene = Scene(ctx, wl.meshes, wl.atlas, wl.sdf_format)
-    fused = not args.plain
-    sess = Session(ctx, session_desc(wl.settings, L.GBUFFER_F32, L.RADIANCE_F32, fused, False))
+    schedule = args.schedule
+    sess = Session(ctx, session_desc(wl.settings, L.GBUFFER_F32, L.RADIANCE_F32, schedule, False))
     stream = torch.cuda.current_stream()
     sh = stream_handle()
 
@@ -324,7 +338,8 @@ def ours(args):
         dist.barrier()
     clk = clocks.stop()
     ms = e0.elapsed_time(e1)
-    stage = np.array([sess.pass_ms(i) for i in range(Wm, Wm + K)])  # [K, 8]
+    ring0 = max(Wm, Wm + K - 128)  # the session keeps events of the last 128 frames
+    stage = np.array([sess.pass_ms(i) for i in range(ring0, Wm + K)])  # [K, 10]
     sess.set_profiling(False)
     assert sess.check() == L.IRT_OK, ctx.error()
     ms_max = ms
@@ -333,28 +348,10 @@ def ours(args):
         dist.all_reduce(tt, op=dist.ReduceOp.MAX)
         ms_max = float(tt.item())
     value = world * P * K / (ms_max / 1000.0) / 1e6
-    frame_ms = stage[:, 7]
-
-    # ---- roofline of the dominant kernel
+    frame_ms = stage[:, 9]
     names = STAGES
-    mean_ms = stage[:, :7].mean(0)
+    mean_ms = stage[:, :9].mean(0)
     kernel_idx = {n: i for i, n in enumerate(names)}
-    candidates = ["reuse", "shade", "svgf_temporal", "svgf_variance", "atrous"]
-    dominant = max(candidates, key=lambda n: mean_ms[kernel_idx[n]])
-    peak, peak_kind = measured_peak()
-
-    def ach(n):
-        return ALG_BYTES[n] * P / (mean_ms[kernel_idx[n]] / 1000.0) / 1e9
-
-    achieved = ach(dominant)
-    traffic = ncu_traffic() if dominant == "shade" else None
-    roofline = {"bound": "hbm", "kernel": dominant, "achieved": achieved, "peak": peak, "unit": "GB/s",
-                "frac": achieved / peak, "traffic": traffic, "peak_source": peak_kind,
-                "alg_bytes_per_pixel": ALG_BYTES[dominant],
-                "kernels": {n: {"ms": float(mean_ms[kernel_idx[n]]), "alg_GBps": ach(n), "frac": ach(n) / peak}
-                            for n in candidates},
-                "note": "shade = spatial reuse + resolve with the SDF soft-shadow march; its time is the "
-                        "march (FP32/latency bound), so its HBM fraction is low by construction"}
 
     # ---- e2e through the C-ABI with host buffers
     e2e = None
@@ -407,23 +404,51 @@ def ours(args):
                "path": "irt_scene_update + irt_render_frame (C-ABI) with pinned host G-buffer and VPL pool "
                        "copied in and the filtered image copied out every step"}
 
-    # ---- CPU baseline (rank 0, N = 1)
-    cpu = None
-    if rank == 0 and world == 1 and not args.no_cpu_baseline:
-        r = cpu_run(spec, 1, 1, args.cpu_seconds)
-        cpu = {"value": r["value"], "unit": "Mpix-frames/s", "cores": r["threads"], "kind": "port",
-               "sample": r["sample"]}
+    # ---- CPU baseline (rank 0, N = 1) and the oracle's work counters
+    cpu, counters = None, None
+    if rank == 0:
+        if world == 1 and not args.no_cpu_baseline:
+            r = cpu_run(spec, 1, 1, args.cpu_seconds)
+            cpu = {"value": r["value"], "unit": "Mpix-frames/s", "cores": r["threads"], "kind": "port",
+                   "sample": r["sample"]}
+        else:
+            r = cpu_run(spec, 1, 1, 1.0)
+        counters = r["counters_per_pixel"]
+
+    # ---- roofline of the dominant kernel
+    dominant = max(KERNELS, key=lambda n: mean_ms[kernel_idx[n]])
+    peak, peak_kind = measured_peak()
+
+    def ach(n):
+        return ALG_BYTES[n] * P / (mean_ms[kernel_idx[n]] / 1000.0) / 1e9
+
+    march_flops = None
+    if counters:
+        march_flops = sum(FLOPS_PER[k] * counters.get(k, 0.0) for k in FLOPS_PER)
+    roofline = {"bound": "hbm", "kernel": dominant, "achieved": ach(dominant), "peak": peak, "unit": "GB/s",
+                "frac": ach(dominant) / peak, "traffic": ncu_traffic(dominant), "peak_source": peak_kind,
+                "alg_bytes_per_pixel": ALG_BYTES[dominant],
+                "kernels": {n: {"ms": float(mean_ms[kernel_idx[n]]), "alg_GBps": ach(n), "frac": ach(n) / peak}
+                            for n in KERNELS}}
+    if march_flops is not None:
+        t = mean_ms[kernel_idx["march"]] / 1000.0
+        roofline["march_fp32"] = {
+            "flops_per_pixel": march_flops, "achieved_tflops": march_flops * P / t / 1e12,
+            "peak_tflops": FP32_PEAK_TFLOPS, "peak_source": "nominal (148 SMs x 128 FP32 lanes x 2 x 1.965 GHz)",
+            "frac": march_flops * P / t / 1e12 / FP32_PEAK_TFLOPS,
+            "counters_per_pixel": counters,
+            "note": "the march is FP32/latency bound; flops counted by the oracle on a band of the same frame"}
 
     if rank == 0:
         line = {
             "metric": "Mpix-frames/s", "value": value, "unit": "Mpix-frames/s", "n_gpus": world, "steps": K,
             "warmup": Wm, "ms_per_step": ms_max / K, "higher_is_better": True, "scaling": "weak",
             "vs_baseline": None, "dtype": "f32", "data": "synthetic",
-            "config": describe(spec, n_frames, "fused" if fused else "plain"),
+            "config": describe(spec, n_frames, {1: "ray-queue", 2: "fused-inline", 0: "plain"}[schedule]),
             "p50_frame_ms": float(np.percentile(frame_ms, 50)), "p99_frame_ms": float(np.percentile(frame_ms, 99)),
             "stage_ms": {n: float(mean_ms[i]) for i, n in enumerate(names)},
             "roofline": roofline, "cpu_baseline": cpu, "e2e": e2e,
-            "gpu_launches": K * (KERNELS_PER_FRAME_FUSED if fused else 14),
+            "gpu_launches": K * {1: KERNELS_PER_FRAME, 2: 8, 0: 14}[schedule],
             "clocks": clk,
         }
         print(json.dumps(line), flush=True)

@@ -203,7 +203,10 @@ typedef struct irt_session_desc {
     int32_t gbuffer_format;
     int32_t radiance_format;
     int32_t moments_format;
-    int32_t fused;            /* 1 = fused kernels (default), 0 = one kernel per reference entry point */
+    int32_t fused;            /* schedule: 1 = candidates+temporal, spatial + ray set-up, persistent
+                                 ray-queue march, resolve combine (default); 2 = candidates+temporal
+                                 and spatial+resolve with the march inline per pixel; 0 = one kernel
+                                 per reference entry point.  All three give identical results. */
     int32_t keep_candidates;  /* 1 = also write the candidates reservoirs [0] (parity/debug) */
 } irt_session_desc;
 
@@ -253,6 +256,8 @@ irt_status irt_render_frame(irt_session* s, const irt_scene* scene, const irt_fr
 #define IRT_BUF_FEEDBACK 10       /* radiance fmt: a-trous-0 output (this)   */
 #define IRT_BUF_FEEDBACK_OLD 11   /* radiance fmt: feedback the next frame reads */
 #define IRT_BUF_ERROR 12          /* u32[4]: device error word (0 = none)    */
+#define IRT_BUF_TEMPORAL 13       /* radiance fmt: svgf_temporal output      */
+#define IRT_BUF_VARIANCE 14       /* radiance fmt: svgf_variance output      */
 /* Device pointer and byte size of one session buffer.  "This frame" refers
  * to the last frame submitted. */
 irt_status irt_session_buffer(irt_session* s, int32_t which, void** ptr, uint64_t* bytes);
@@ -266,11 +271,12 @@ irt_status irt_session_check(irt_session* s, void* stream);
 /* Device time of the last frame's passes (ms), measured with CUDA events
  * when profiling is on: names as in src/renderer.rs:2077-2092. */
 irt_status irt_session_set_profiling(irt_session* s, int32_t on);
-/* Stages: archive copy, candidates+temporal, spatial+resolve, SVGF temporal,
- * SVGF variance, a-trous, history copy, total.  Events are kept for the last
- * 128 frames, so a timed run is read back after it ends. */
-irt_status irt_session_pass_ms(irt_session* s, float out_ms[8]);
-irt_status irt_session_pass_ms_at(irt_session* s, uint32_t frame_index, float out_ms[8]);
+/* Ten values: archive copy, candidates+temporal, spatial (+ ray set-up),
+ * march, resolve combine, SVGF temporal, SVGF variance, a-trous, history
+ * copy, total.  Events are kept for the last 128 frames, so a timed run is
+ * read back after it ends. */
+irt_status irt_session_pass_ms(irt_session* s, float out_ms[10]);
+irt_status irt_session_pass_ms_at(irt_session* s, uint32_t frame_index, float out_ms[10]);
 
 /* ---------------------------------------------------------------------------
  * Host logic of src/renderer.rs used to build scene data (C++ equivalents).

@@ -32,6 +32,7 @@ BUF_DIRECT, BUF_NOISY, BUF_FILTERED, BUF_MOMENTS = 0, 1, 2, 3
 BUF_RES_DIRECT, BUF_RES_INDIRECT, BUF_VPL_ARCHIVE = 4, 5, 6
 BUF_PREV_DEPTH, BUF_PREV_NORMAL, BUF_MOMENTS_OLD = 7, 8, 9
 BUF_FEEDBACK, BUF_FEEDBACK_OLD, BUF_ERROR = 10, 11, 12
+BUF_TEMPORAL, BUF_VARIANCE = 13, 14
 
 
 class Mat4(C.Structure):

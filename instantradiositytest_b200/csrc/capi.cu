@@ -11,6 +11,7 @@
 #include <string>
 #include <vector>
 
+#include "dev_sdf.cuh"
 #include "kernels.h"
 #include "workload.h"
 
@@ -40,6 +41,14 @@ struct irt_scene {
     irt_node* nodes = nullptr;
     irt_light* lights = nullptr;
     uint32_t object_cap = 0, light_cap = 0;
+    // compact march scene (nodes + object records with their mesh folded in)
+    float4* march_scene = nullptr;
+    std::vector<float4> march_host;
+    // leaf-order cache (rebuilt when the BVH changes)
+    uint4* cells = nullptr;
+    std::vector<uint32_t> cells_host;
+    std::vector<irt_node> cached_nodes;
+    float grid_org[3] = {0, 0, 0}, grid_inv[3] = {0, 0, 0};
     uint32_t object_count = 0, light_count = 0;
     uint64_t bytes = 0;
 };
@@ -70,7 +79,14 @@ struct irt_session {
     // Profiling: a ring of kProfRing frames x 8 stage-boundary events, so a
     // long timed run can be read back afterwards without per-frame syncs.
     static constexpr int kProfRing = 128;
-    cudaEvent_t ev[kProfRing][8] = {};
+    static constexpr int kProfEvents = 10;
+    cudaEvent_t ev[kProfRing][kProfEvents] = {};
+    // ray-queue resolve buffers
+    RayRecord* rays = nullptr;
+    uint32_t* ray_counters = nullptr;
+    float* vis = nullptr;
+    float4* pending = nullptr;
+    int num_sms = 0;
     bool ev_ready = false;
     int prof_slot = 0;
     uint32_t prof_frame[kProfRing] = {};
@@ -239,6 +255,10 @@ irt_status irt_scene_update(irt_scene* sc, const irt_object* objects, uint32_t o
         ctx->set_error("scene update needs objects and 2N-1 nodes");
         return IRT_E_INVALID;
     }
+    if (object_count > kMaxMarchObjects) {
+        ctx->set_error("more objects than the march scene holds (1024)");
+        return IRT_E_INVALID;
+    }
     // Validate every index the device walk follows: mesh ids, leaf object
     // ids, and escape links that strictly advance and stay within 2N-1.
     for (uint32_t i = 0; i < object_count; i++)
@@ -284,6 +304,67 @@ irt_status irt_scene_update(irt_scene* sc, const irt_object* objects, uint32_t o
     CK(cudaMemcpyAsync(sc->nodes, nodes, sizeof(irt_node) * node_count, cudaMemcpyHostToDevice, st), "nodes");
     if (light_count)
         CK(cudaMemcpyAsync(sc->lights, lights, sizeof(irt_light) * light_count, cudaMemcpyHostToDevice, st), "lights");
+    // Compact march scene: the same values, laid out for shared memory.
+    const uint32_t mbytes = irt_march_scene_bytes(object_count);
+    if (sc->march_host.size() * 16 < mbytes) {
+        if (sc->march_scene) cudaFree(sc->march_scene);
+        sc->march_scene = nullptr;
+        uint64_t added = 0;
+        irt_status s1 = dev_alloc(ctx, &sc->march_scene, mbytes, added);
+        if (s1) return s1;
+        sc->bytes += added;
+        ctx->in_use += added;
+    }
+    sc->march_host.assign(mbytes / 16, make_float4(0.f, 0.f, 0.f, 0.f));
+    irtd::MNode* mn = reinterpret_cast<irtd::MNode*>(sc->march_host.data());
+    irtd::MObj* mo = reinterpret_cast<irtd::MObj*>(mn + node_count);
+    auto bits = [](uint32_t u) {
+        float f;
+        std::memcpy(&f, &u, 4);
+        return f;
+    };
+    std::vector<uint32_t> leaf_of(object_count, 0);
+    for (uint32_t i = 0; i < node_count; i++) {
+        const irt_node& n = nodes[i];
+        mn[i].a = make_float4(n.lo[0], n.lo[1], n.lo[2], bits(n.info[3]));
+        mn[i].b = make_float4(n.hi[0], n.hi[1], n.hi[2], bits(n.info[2] == 1u ? n.info[0] : 0xffffffffu));
+        if (n.info[2] == 1u) leaf_of[n.info[0]] = i;
+    }
+    for (uint32_t i = 0; i < object_count; i++) {
+        const irt_object& o = objects[i];
+        const irt_mesh& m = sc->host_meshes[o.info[0]];
+        const float* inv = o.inverse.m;  // column-major
+        mo[i].rx = make_float4(inv[0], inv[4], inv[8], inv[12]);
+        mo[i].ry = make_float4(inv[1], inv[5], inv[9], inv[13]);
+        mo[i].rz = make_float4(inv[2], inv[6], inv[10], inv[14]);
+        mo[i].meta = make_float4(bits(o.info[2]), bits(o.info[3]), bits(o.info[0]), bits(leaf_of[i]));
+        mo[i].lo = make_float4(m.lo[0], m.lo[1], m.lo[2], m.lo[3]);
+        mo[i].hi = make_float4(m.hi[0], m.hi[1], m.hi[2], m.hi[3]);
+        mo[i].field = make_uint4(m.field[0], m.field[1], m.field[2], m.field[3]);
+        mo[i].grid = make_float4(m.grid[0], m.grid[1], m.grid[2], m.grid[3]);
+        mo[i].glo = make_float4(m.geometry_lo[0], m.geometry_lo[1], m.geometry_lo[2], m.geometry_lo[3]);
+        mo[i].ghi = make_float4(m.geometry_hi[0], m.geometry_hi[1], m.geometry_hi[2], m.geometry_hi[3]);
+        mo[i].sphere = make_float4(m.enclosing_sphere[0], m.enclosing_sphere[1], m.enclosing_sphere[2],
+                                   m.enclosing_sphere[3]);
+    }
+    CK(cudaMemcpyAsync(sc->march_scene, sc->march_host.data(), mbytes, cudaMemcpyHostToDevice, st), "march scene");
+    // Leaf-order cache, rebuilt only when the BVH changes (static scenes
+    // build it once).
+    if (sc->cached_nodes.size() != node_count ||
+        std::memcmp(sc->cached_nodes.data(), nodes, sizeof(irt_node) * node_count) != 0) {
+        const size_t words = (size_t)kGridRes * kGridRes * kGridRes * kCellWords;
+        if (!sc->cells) {
+            uint64_t added = 0;
+            irt_status s1 = dev_alloc(ctx, &sc->cells, words * 4, added);
+            if (s1) return s1;
+            sc->bytes += added;
+            ctx->in_use += added;
+        }
+        sc->cells_host.assign(words, 0u);
+        irt_build_leaf_cache(nodes, object_count, sc->cells_host.data(), sc->grid_org, sc->grid_inv);
+        CK(cudaMemcpyAsync(sc->cells, sc->cells_host.data(), words * 4, cudaMemcpyHostToDevice, st), "leaf cache");
+        sc->cached_nodes.assign(nodes, nodes + node_count);
+    }
     sc->object_count = object_count;
     sc->light_count = light_count;
     return IRT_OK;
@@ -298,6 +379,8 @@ void irt_scene_destroy(irt_scene* sc) {
     if (sc->objects) cudaFree(sc->objects);
     if (sc->nodes) cudaFree(sc->nodes);
     if (sc->lights) cudaFree(sc->lights);
+    if (sc->march_scene) cudaFree(sc->march_scene);
+    if (sc->cells) cudaFree(sc->cells);
     if (sc->ctx->in_use >= sc->bytes) sc->ctx->in_use -= sc->bytes;
     delete sc;
 }
@@ -316,6 +399,7 @@ uint64_t irt_session_bytes(const irt_session_desc* d) {
     b += P * rad * 7;  // noisy, feedback x2, temporal, scratch x2, filtered
     b += P * 16 * 2;   // moments x2
     b += 16;           // error word
+    if (d->fused == 1) b += P * (2 * sizeof(RayRecord) + 2 * 4 + 2 * 16) + 16;  // ray queue, vis, pending
     return b;
 }
 
@@ -383,6 +467,14 @@ irt_status irt_session_create(irt_context* ctx, const irt_session_desc* desc, ir
     if (!st) st = dev_alloc(ctx, &s->temporal, P * s->rad_bytes, used);
     if (!st) st = dev_alloc(ctx, &s->filtered, P * s->rad_bytes, used);
     if (!st) st = dev_alloc(ctx, &s->error, 16, used);
+    if (desc->fused == 1) {
+        if (!st) st = dev_alloc(ctx, &s->rays, P * 2 * sizeof(RayRecord), used);
+        if (!st) st = dev_alloc(ctx, &s->ray_counters, 16, used);
+        if (!st) st = dev_alloc(ctx, &s->vis, P * 2 * 4, used);
+        if (!st) st = dev_alloc(ctx, &s->pending, P * 2 * 16, used);
+    }
+    if (!st && cudaDeviceGetAttribute(&s->num_sms, cudaDevAttrMultiProcessorCount, ctx->device) != cudaSuccess)
+        st = IRT_E_CUDA;
     if (st) return fail(st);
     *out = s;
     return IRT_OK;
@@ -393,7 +485,8 @@ void irt_session_destroy(irt_session* s) {
     DeviceGuard g(s->ctx->device);
     void* ptrs[] = {s->dres[0], s->dres[1], s->dres[2], s->ires[0], s->ires[1], s->ires[2], s->archive,
                     s->prev_depth, s->prev_normal, s->direct, s->noisy, s->moments[0], s->moments[1],
-                    s->feedback[0], s->feedback[1], s->temporal, s->scratch[0], s->scratch[1], s->filtered, s->error};
+                    s->feedback[0], s->feedback[1], s->temporal, s->scratch[0], s->scratch[1], s->filtered, s->error,
+                    s->rays, s->ray_counters, s->vis, s->pending};
     for (void* p : ptrs)
         if (p) cudaFree(p);
     if (s->ev_ready)
@@ -480,16 +573,55 @@ irt_status irt_frame_lighting(irt_session* s, const irt_scene* sc, const irt_fra
     L.noisy_out = s->noisy;
     L.radiance_f16 = s->desc.radiance_format == IRT_RADIANCE_F16;
     L.keep_candidates = s->desc.keep_candidates;
-    if (s->desc.fused) {
+    L.rays = s->rays;
+    L.ray_counters = s->ray_counters;
+    L.vis = s->vis;
+    L.pending = s->pending;
+    if (s->desc.fused == 1) {
+        // candidates+temporal -> spatial + resolve set-up (ray queue) ->
+        // persistent march -> resolve outputs.
+        CK(cudaMemsetAsync(s->ray_counters, 0, 16, st), "ray counters");
+        CK(irt_launch_lighting(L, kStageReuse, st), "reuse kernel");
+        mark(s, 2, st);
+        CK(irt_launch_lighting(L, kStageSpatial, st), "spatial kernel");
+        mark(s, 3, st);
+        MarchLaunch M{};
+        M.frame = f;
+        M.objects = sc->objects;
+        M.meshes = sc->meshes;
+        M.nodes = sc->nodes;
+        M.atlas = sc->atlas;
+        M.sdf_f16 = sc->sdf_f16;
+        M.error = s->error;
+        M.march_scene = sc->march_scene;
+        M.cells = sc->cells;
+        for (int a = 0; a < 3; a++) {
+            M.grid_org[a] = sc->grid_org[a];
+            M.grid_inv[a] = sc->grid_inv[a];
+        }
+        M.rays = s->rays;
+        M.ray_counters = s->ray_counters;
+        M.vis = s->vis;
+        M.num_sms = s->num_sms;
+        CK(irt_launch_march(M, st), "march kernel");
+        mark(s, 4, st);
+        CK(irt_launch_lighting(L, kStageCombine, st), "combine kernel");
+        mark(s, 5, st);
+    } else if (s->desc.fused == 2) {
         CK(irt_launch_lighting(L, kStageReuse, st), "reuse kernel");
         mark(s, 2, st);
         CK(irt_launch_lighting(L, kStageShade, st), "shade kernel");
         mark(s, 3, st);
+        mark(s, 4, st);
+        mark(s, 5, st);
     } else {
         for (int p = 0; p < 4; p++) CK(irt_launch_lighting(L, p, st), "lighting pass");
         mark(s, 2, st);
-        for (int p = 4; p < 8; p++) CK(irt_launch_lighting(L, p, st), "lighting pass");
+        for (int p = 4; p < 6; p++) CK(irt_launch_lighting(L, p, st), "lighting pass");
         mark(s, 3, st);
+        for (int p = 6; p < 8; p++) CK(irt_launch_lighting(L, p, st), "lighting pass");
+        mark(s, 4, st);
+        mark(s, 5, st);
     }
     s->last_frame = f->size[2];
     s->have_frame = true;
@@ -507,9 +639,9 @@ irt_status irt_frame_svgf(irt_session* s, const irt_frame* f, const irt_gbuffer*
     const size_t rb = s->P * s->rad_bytes;
     if (f->flags[2] >= 3u) {  // debug views bypass SVGF (src/svgf.rs:154-161)
         CK(cudaMemcpyAsync(s->filtered, s->noisy, rb, cudaMemcpyDeviceToDevice, st), "svgf bypass");
-        mark(s, 4, st);
-        mark(s, 5, st);
         mark(s, 6, st);
+        mark(s, 7, st);
+        mark(s, 8, st);
     } else {
         SvgfLaunch L{};
         L.frame = f;
@@ -523,12 +655,12 @@ irt_status irt_frame_svgf(irt_session* s, const irt_frame* f, const irt_gbuffer*
         L.out = s->temporal;
         L.moments_out = s->moments[cur];
         CK(irt_launch_svgf(L, 0, st), "svgf temporal");
-        mark(s, 4, st);
+        mark(s, 6, st);
         L.in = s->temporal;
         L.moments_in = s->moments[cur];
         L.out = s->scratch[0];
         CK(irt_launch_svgf(L, 1, st), "svgf variance");
-        mark(s, 5, st);
+        mark(s, 7, st);
         // A-trous ping-pong: iteration 0 writes feedback[cur] directly (the
         // reference copies scratch[1] there), the last writes the output.
         const uint32_t iters = s->desc.settings.svgf_iterations;
@@ -549,13 +681,13 @@ irt_status irt_frame_svgf(irt_session* s, const irt_frame* f, const irt_gbuffer*
             CK(irt_launch_svgf(L, 2, st), "svgf atrous");
             in = out;
         }
-        mark(s, 6, st);
+        mark(s, 8, st);
     }
     // Depth/normal history for the next frame (src/renderer.rs:1951-1960).
     CK(cudaMemcpyAsync(s->prev_depth, g->depth, s->P * 4, cudaMemcpyDeviceToDevice, st), "depth history");
     CK(cudaMemcpyAsync(s->prev_normal, g->normal, s->P * s->normal_bytes, cudaMemcpyDeviceToDevice, st),
        "normal history");
-    mark(s, 7, st);
+    mark(s, 9, st);
     return IRT_OK;
 }
 
@@ -587,6 +719,8 @@ irt_status irt_session_buffer(irt_session* s, int32_t which, void** ptr, uint64_
     case IRT_BUF_PREV_DEPTH: p = s->prev_depth; b = P * 4; break;
     case IRT_BUF_PREV_NORMAL: p = s->prev_normal; b = P * s->normal_bytes; break;
     case IRT_BUF_ERROR: p = s->error; b = 16; break;
+    case IRT_BUF_TEMPORAL: p = s->temporal; b = P * s->rad_bytes; break;
+    case IRT_BUF_VARIANCE: p = s->scratch[0]; b = P * s->rad_bytes; break;
     default: break;
     }
     if (which == IRT_BUF_RES_DIRECT || which == IRT_BUF_RES_INDIRECT) {
@@ -637,7 +771,7 @@ irt_status irt_session_set_profiling(irt_session* s, int32_t on) {
 // temporal, spatial + resolve, SVGF temporal, SVGF variance, a-trous,
 // history copy, total.  Synchronises on that frame's last event.  Frames
 // older than the ring (128 frames) are overwritten.
-irt_status irt_session_pass_ms_at(irt_session* s, uint32_t frame_index, float out_ms[8]) {
+irt_status irt_session_pass_ms_at(irt_session* s, uint32_t frame_index, float out_ms[10]) {
     if (!s || !out_ms || !s->ev_ready) return IRT_E_STATE;
     irt_context* ctx = s->ctx;
     int slot = (int)(frame_index % irt_session::kProfRing);
@@ -647,13 +781,14 @@ irt_status irt_session_pass_ms_at(irt_session* s, uint32_t frame_index, float ou
     }
     DeviceGuard dg(ctx->device);
     cudaEvent_t* e = s->ev[slot];
-    CK(cudaEventSynchronize(e[7]), "event sync");
-    for (int k = 0; k < 7; k++) CK(cudaEventElapsedTime(&out_ms[k], e[k], e[k + 1]), "elapsed");
-    CK(cudaEventElapsedTime(&out_ms[7], e[0], e[7]), "elapsed");
+    const int last = irt_session::kProfEvents - 1;
+    CK(cudaEventSynchronize(e[last]), "event sync");
+    for (int k = 0; k < last; k++) CK(cudaEventElapsedTime(&out_ms[k], e[k], e[k + 1]), "elapsed");
+    CK(cudaEventElapsedTime(&out_ms[last], e[0], e[last]), "elapsed");
     return IRT_OK;
 }
 
-irt_status irt_session_pass_ms(irt_session* s, float out_ms[8]) {
+irt_status irt_session_pass_ms(irt_session* s, float out_ms[10]) {
     if (!s) return IRT_E_INVALID;
     return irt_session_pass_ms_at(s, s->last_frame, out_ms);
 }

@@ -116,15 +116,37 @@ __device__ __forceinline__ float mesh_distance(const DevScene& sc, V3 p, const D
 }
 
 // sdf.wgsl:35-41 (returns the distance; the voxel is selected by the caller).
-__device__ __forceinline__ float object_distance(const DevScene& sc, V3 p, const DObject& o) {
-    V3 local = V3{o.c0.x * p.x + o.c1.x * p.y + o.c2.x * p.z + o.c3.x,
-                  o.c0.y * p.x + o.c1.y * p.y + o.c2.y * p.z + o.c3.y,
-                  o.c0.z * p.x + o.c1.z * p.y + o.c2.z * p.z + o.c3.z};
-    DMesh mesh = load_mesh(sc.meshes, o.info.x);
-    float d = mesh_distance(sc, local, mesh) * __uint_as_float(o.info.z);
+// rx/ry/rz are the rows of the object's inverse matrix.
+__device__ __forceinline__ float object_distance_rows(const DevScene& sc, V3 p, float4 rx, float4 ry, float4 rz,
+                                                      float scale, const DMesh& mesh) {
+    V3 local = V3{rx.x * p.x + rx.y * p.y + rx.z * p.z + rx.w, ry.x * p.x + ry.y * p.y + ry.z * p.z + ry.w,
+                  rz.x * p.x + rz.y * p.y + rz.z * p.z + rz.w};
+    float d = mesh_distance(sc, local, mesh) * scale;
     if (d > 0.f) d *= .9999f;
     return d;
 }
+__device__ __forceinline__ float object_distance(const DevScene& sc, V3 p, const DObject& o) {
+    DMesh mesh = load_mesh(sc.meshes, o.info.x);
+    return object_distance_rows(sc, p, make_float4(o.c0.x, o.c1.x, o.c2.x, o.c3.x),
+                                make_float4(o.c0.y, o.c1.y, o.c2.y, o.c3.y), make_float4(o.c0.z, o.c1.z, o.c2.z, o.c3.z),
+                                __uint_as_float(o.info.z), mesh);
+}
+
+// Compact per-frame march scene (built on the host by irt_scene_update):
+// preorder nodes then one record per object with its mesh folded in.
+struct MNode {
+    float4 a;  // lo.xyz, bits(escape index)
+    float4 b;  // hi.xyz, bits(object id) for leaves, 0xffffffff otherwise
+};
+struct MObj {
+    float4 rx, ry, rz;  // rows of the inverse model matrix
+    float4 meta;        // bits(scale), bits(voxel diagonal * scale), mesh id, 0
+    float4 lo, hi;      // mesh SDF bounds (lo.w: f16 texel scale)
+    uint4 field;
+    float4 grid, glo, ghi, sphere;
+};
+static_assert(sizeof(MNode) == 32, "MNode layout");
+static_assert(sizeof(MObj) == 176, "MObj layout");
 
 struct Dist {
     float best, voxel;
@@ -134,8 +156,8 @@ struct Dist {
 // sdf.wgsl:42-60 — the cursor only moves forward (escape links point past
 // the subtree), so a walk visits at most 2N-1 nodes; a link that does not
 // advance is reported through the error word and ends the walk.
-template <bool NeedSpacing>
-__device__ __forceinline__ Dist scene_distance(const DevScene& sc, const irt_frame& f, V3 p, uint32_t hint) {
+__device__ __forceinline__ Dist scene_distance(const DevScene& sc, const irt_frame& f, V3 p, uint32_t hint,
+                                               bool NeedSpacing) {
     Dist r{1e20f, f.sdf[1], hint};
     const uint32_t n = f.counts[3];
     if (hint < n) {
@@ -176,39 +198,67 @@ __device__ __forceinline__ Dist scene_distance(const DevScene& sc, const irt_fra
     return r;
 }
 
+// The march of sdf.wgsl:61-81 split into steps shared by the per-pixel
+// visibility() and the ray-queue march kernel, so both evaluate the same
+// operations.  Each returns the resolved visibility, or -1 to continue.
+struct MarchState {
+    V3 origin, dir;
+    float t, limit, result, previous;
+    uint32_t closest, step;
+};
+// Top of march iteration `step`: budget first, then the ray length.
+__device__ __forceinline__ float march_top(const MarchState& m, uint32_t max_steps) {
+    if (m.step >= max_steps) return 0.f;  // a budget-exhausted ray is unresolved
+    if (m.t >= m.limit) return wclamp(m.result, 0.f, 1.f);
+    return -1.f;
+}
+__device__ __forceinline__ float march_begin(MarchState& m, V3 endpoint, float eps, uint32_t max_steps) {
+    V3 delta = endpoint - m.origin;
+    m.limit = length(delta) - eps;
+    if (m.limit <= 0.f) return 1.f;
+    m.dir = normalize(delta);
+    m.t = eps;
+    m.result = 1.f;
+    m.previous = 1e20f;
+    m.step = 0;
+    return march_top(m, max_steps);
+}
+__device__ __forceinline__ V3 march_point(const MarchState& m) { return m.origin + m.dir * m.t; }
+// Quilez improved penumbra update after a query of distance h.
+__device__ __forceinline__ float march_after(MarchState& m, float h, float eps, float k, uint32_t max_steps) {
+    if (h < eps) return 0.f;
+    float y = h * h / (2.f * m.previous);
+    float d = sqrtf(wmax(h * h - y * y, 0.f));
+    if (m.t > y) m.result = wmin(m.result, k * d / (m.t - y));
+    if (m.result < .001f) return 0.f;
+    m.previous = h;
+    m.t += h;
+    m.step++;
+    return march_top(m, max_steps);
+}
+__device__ __forceinline__ float clearance_epsilon(float eps, float voxel) { return wmax(eps, voxel * .65f); }
+
 // sdf.wgsl:61-81 — soft-shadow visibility of `target` from surface point p.
 __device__ __forceinline__ float visibility(const DevScene& sc, const irt_frame& f, V3 p, V3 n, V3 target,
                                             V3 end_normal) {
     const float eps = f.sdf[1];
-    Dist clearance = scene_distance<true>(sc, f, p, 0xffffffffu);
-    float epsilon = wmax(eps, clearance.voxel * .65f);
-    uint32_t closest = clearance.closest;
-    V3 origin = p + n * epsilon;
+    const uint32_t steps = to_u32(f.sdf[0]);
+    MarchState m;
+    Dist clearance = scene_distance(sc, f, p, 0xffffffffu, true);
+    m.closest = clearance.closest;
+    m.origin = p + n * clearance_epsilon(eps, clearance.voxel);
     V3 endpoint = target;
     if (dot(end_normal, end_normal) > .5f) {
-        Dist e = scene_distance<true>(sc, f, target, 0xffffffffu);
-        endpoint = endpoint + end_normal * wmax(eps, e.voxel * .65f);
+        Dist e = scene_distance(sc, f, target, 0xffffffffu, true);
+        endpoint = target + end_normal * clearance_epsilon(eps, e.voxel);
     }
-    V3 delta = endpoint - origin;
-    float limit = length(delta) - eps;
-    if (limit <= 0.f) return 1.f;
-    V3 direction = normalize(delta);
-    float t = eps, result = 1.f, previous = 1e20f;
-    const uint32_t steps = to_u32(f.sdf[0]);
-    for (uint32_t i = 0; i < steps; i++) {
-        if (t >= limit) return wclamp(result, 0.f, 1.f);
-        Dist q = scene_distance<false>(sc, f, origin + direction * t, closest);
-        float h = q.best;
-        closest = q.closest;
-        if (h < eps) return 0.f;
-        float y = h * h / (2.f * previous);
-        float d = sqrtf(wmax(h * h - y * y, 0.f));
-        if (t > y) result = wmin(result, f.sdf[2] * d / (t - y));
-        if (result < .001f) return 0.f;
-        previous = h;
-        t += h;
+    float r = march_begin(m, endpoint, eps, steps);
+    while (r < 0.f) {
+        Dist q = scene_distance(sc, f, march_point(m), m.closest, false);
+        m.closest = q.closest;
+        r = march_after(m, q.best, eps, f.sdf[2], steps);
     }
-    return 0.f;
+    return r;
 }
 
 }  // namespace irtd

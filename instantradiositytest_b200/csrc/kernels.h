@@ -7,8 +7,18 @@
 // Lighting stages: 0..7 are the reference entry points in schedule order
 // (candidates_direct, candidates_indirect, temporal_direct, temporal_indirect,
 // spatial_direct, spatial_indirect, resolve_direct, resolve_indirect).
-constexpr int kStageReuse = 100;  // fused 0..3
-constexpr int kStageShade = 101;  // fused 4..7
+constexpr int kStageReuse = 100;    // fused 0..3
+constexpr int kStageShade = 101;    // fused 4..7 with the march inline (one thread per pixel)
+constexpr int kStageSpatial = 102;  // fused 4..5 + resolve set-up: emits visibility rays
+constexpr int kStageCombine = 103;  // resolve 6..7 from contributions x visibility
+
+// A visibility ray of the resolve passes (sdf.wgsl:61-81 arguments), 64 bytes:
+//   a = (p.xyz, bits(pixel * 2 + kind))  kind 0 = direct, 1 = indirect
+//   b = (n.xyz, 1 if the endpoint is offset along end_normal else 0)
+//   c = (target.xyz, 0), d = (end_normal.xyz, 0)
+struct RayRecord {
+    float4 a, b, c, d;
+};
 
 struct LightingLaunch {
     const irt_frame* frame;
@@ -31,7 +41,48 @@ struct LightingLaunch {
     void* noisy_out;
     int radiance_f16;
     int keep_candidates;
+    // ray-queue resolve (kStageSpatial / march / kStageCombine)
+    RayRecord* rays;         // capacity 2 * W * H
+    uint32_t* ray_counters;  // [0] rays emitted, [1] rays fetched by the march
+    float* vis;              // visibility per pixel * 2 + kind
+    float4* pending;         // per pixel: direct contribution (w = 1: x vis), indirect (w = 1: x vis)
 };
+
+struct MarchLaunch {
+    const irt_frame* frame;
+    const irt_object* objects;
+    const irt_mesh* meshes;
+    const irt_node* nodes;
+    cudaTextureObject_t atlas;
+    int sdf_f16;
+    uint32_t* error;
+    const float4* march_scene;  // compact nodes + objects (irt_march_scene_bytes)
+    // Leaf-order cache: a kGridRes^3 grid over the root box; per cell the
+    // first kCellEntries objects by increasing distance from the cell to their
+    // BVH leaf box, with those distances and the next one as a sentinel.
+    const uint4* cells;
+    float grid_org[3], grid_inv[3];
+    const RayRecord* rays;
+    uint32_t* ray_counters;
+    float* vis;
+    int num_sms;
+};
+cudaError_t irt_launch_march(const MarchLaunch& M, cudaStream_t st);
+// Bytes of the compact march scene of `object_count` objects: 2N-1 nodes of
+// 32 bytes, then N object records of 176 bytes (mesh folded in).
+uint32_t irt_march_scene_bytes(uint32_t object_count);
+constexpr uint32_t kMaxMarchObjects = 1024;  // the march scene lives in shared memory
+constexpr uint32_t kGridRes = 32;
+constexpr uint32_t kCellEntries = 8;
+// One cell: 4 x uint4 = ids (8 x u16 in words 0-3), lower bounds (f32 words
+// 4-11), sentinel bound of the first object left out (word 12), pad.
+constexpr uint32_t kCellWords = 16;
+// Builds the leaf-order cache from the BVH nodes (host, OpenMP): grid over
+// the root box, per cell the kCellEntries objects whose leaf boxes are
+// nearest to the cell (distance to the cell grown by a rounding margin,
+// rounded toward zero and scaled by .9998), then the next bound.  `cells`
+// receives kGridRes^3 * kCellWords words.
+void irt_build_leaf_cache(const irt_node* nodes, uint32_t object_count, uint32_t* cells, float org[3], float inv[3]);
 
 struct SvgfLaunch {
     const irt_frame* frame;

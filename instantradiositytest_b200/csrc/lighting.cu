@@ -31,6 +31,10 @@ struct LightArgs {
     irt_reservoir* ires[3];
     float4* direct_out;  // resolve_direct output (f32x4), may be null in fused mode
     void* noisy_out;     // resolve_indirect output (radiance format)
+    RayRecord* rays;
+    uint32_t* ray_counters;
+    const float* vis;
+    float4* pending;
 };
 
 template <class G>
@@ -276,6 +280,107 @@ __global__ void __launch_bounds__(256) shade_kernel(const __grid_constant__ irt_
     store_noisy<R>(a.noisy_out, px.id, total);
 }
 
+// ---------------------------------------------------------------- ray-queue resolve
+// spatial_direct + spatial_indirect, then the resolve passes up to their
+// visibility call: the pixel's contribution value * normalization is stored
+// and, where the reference would march, a ray is appended to the queue
+// (warp-aggregated: one atomic per warp).  Lanes of out-of-image pixels stay
+// in the warp until the append so every shuffle sees all 32 lanes.
+template <class G, class R>
+__global__ void __launch_bounds__(256) spatial_prep_kernel(const __grid_constant__ irt_frame f,
+                                                           const __grid_constant__ LightArgs<G> a) {
+    uint32_t x = blockIdx.x * blockDim.x + threadIdx.x;
+    uint32_t y = blockIdx.y * blockDim.y + threadIdx.y;
+    const bool in = x < f.size[0] && y < f.size[1];
+    RayRecord ray[2];
+    int n_rays = 0;
+    size_t id = 0;
+    if (in) {
+        Px<G> px(f, a, x, y);
+        id = px.id;
+        bool ok = px.valid();
+        Surface s;
+        if (ok) s = px.surface();
+        Res rd = px.template spatial<0>(res_load(a.dres[1], px.id), ok, s);
+        res_store(a.dres[2], px.id, rd);
+        Res ri = px.template spatial<1>(res_load(a.ires[1], px.id), ok, s);
+        res_store(a.ires[2], px.id, ri);
+        // resolve_direct (lighting.wgsl:106-122) up to visibility()
+        float4 pd = make_float4(0.f, 0.f, 0.f, 0.f);
+        uint32_t dbg = f.flags[2];
+        if (ok) {
+            if (rd.target > 0.f && dbg != 2u && dbg < 3u) {
+                DLight l = load_light(a.sc.lights, rd.id);
+                V3 value = direct(s, l, px.camera());
+                if (luminance(value) > 0.f) {
+                    float k = normalization(rd);
+                    pd = make_float4(value.x * k, value.y * k, value.z * k, 1.f);
+                    ray[n_rays].a = make_float4(s.p.x, s.p.y, s.p.z, __uint_as_float((uint32_t)(id * 2)));
+                    ray[n_rays].b = make_float4(s.n.x, s.n.y, s.n.z, 0.f);
+                    ray[n_rays].c = make_float4(l.ps.x, l.ps.y, l.ps.z, 0.f);
+                    ray[n_rays].d = make_float4(0.f, 0.f, 0.f, 0.f);
+                    n_rays++;
+                }
+            }
+            if (dbg == 3u) pd = make_float4(s.color.x, s.color.y, s.color.z, 0.f);
+            if (dbg == 4u) pd = make_float4(s.n.x * .5f + .5f, s.n.y * .5f + .5f, s.n.z * .5f + .5f, 0.f);
+            if (dbg == 5u) {
+                float2 m = a.g.mv(px.id);
+                pd = make_float4(wclamp(.5f + m.x * 50.f, 0.f, 1.f), wclamp(.5f + m.y * 50.f, 0.f, 1.f), .5f, 0.f);
+            }
+        }
+        // resolve_indirect (lighting.wgsl:123-134) up to visibility()
+        float4 pi = make_float4(0.f, 0.f, 0.f, 0.f);
+        if (ok && dbg != 1u && dbg < 3u && px.vpl_sample_valid(ri)) {
+            DVpl smp = px.selected_vpl(ri);
+            V3 value = indirect(s, smp, px.camera());
+            if (luminance(value) > 0.f) {
+                float k = normalization(ri);
+                pi = make_float4(value.x * k, value.y * k, value.z * k, 1.f);
+                ray[n_rays].a = make_float4(s.p.x, s.p.y, s.p.z, __uint_as_float((uint32_t)(id * 2 + 1)));
+                ray[n_rays].b = make_float4(s.n.x, s.n.y, s.n.z, 1.f);
+                ray[n_rays].c = make_float4(smp.pos.x, smp.pos.y, smp.pos.z, 0.f);
+                ray[n_rays].d = make_float4(smp.nrm.x, smp.nrm.y, smp.nrm.z, 0.f);
+                n_rays++;
+            }
+        }
+        a.pending[id * 2] = pd;
+        a.pending[id * 2 + 1] = pi;
+    }
+    // Warp-aggregated append.
+    const unsigned full = 0xffffffffu;
+    const int lane = threadIdx.x & 31;
+    int incl = n_rays;
+#pragma unroll
+    for (int o = 1; o < 32; o <<= 1) {
+        int t = __shfl_up_sync(full, incl, o);
+        if (lane >= o) incl += t;
+    }
+    int total = __shfl_sync(full, incl, 31);
+    uint32_t base = 0;
+    if (lane == 31 && total > 0) base = atomicAdd(a.ray_counters, (uint32_t)total);
+    base = __shfl_sync(full, base, 31);
+    uint32_t slot = base + (uint32_t)(incl - n_rays);
+    for (int k = 0; k < n_rays; k++) a.rays[slot + k] = ray[k];
+}
+
+// resolve_direct / resolve_indirect outputs from contribution x visibility:
+// direct = c_d * vis_d (or the debug colour), noisy = min(direct + c_i * vis_i, 65000).
+template <class R>
+__global__ void __launch_bounds__(256) combine_kernel(const __grid_constant__ irt_frame f, const float4* pending,
+                                                      const float* vis, float4* direct_out, void* noisy_out) {
+    size_t i = (size_t)blockIdx.x * blockDim.x + threadIdx.x;
+    size_t P = (size_t)f.size[0] * f.size[1];
+    if (i >= P) return;
+    float4 pd = pending[i * 2], pi = pending[i * 2 + 1];
+    float2 v = reinterpret_cast<const float2*>(vis)[i];
+    V3 result = V3{pd.x, pd.y, pd.z};
+    if (pd.w != 0.f) result = V3{pd.x * v.x, pd.y * v.x, pd.z * v.x};
+    direct_out[i] = make_float4(result.x, result.y, result.z, 1.f);
+    if (pi.w != 0.f) result = result + V3{pi.x * v.y, pi.y * v.y, pi.z * v.y};
+    store_noisy<R>(noisy_out, i, result);
+}
+
 // ---------------------------------------------------------------- plain kernels
 template <class G, class R, int Pass>
 __global__ void __launch_bounds__(256) pass_kernel(const __grid_constant__ irt_frame f, const __grid_constant__ LightArgs<G> a) {
@@ -344,6 +449,10 @@ static LightArgs<G> make_args(const LightingLaunch& L) {
     }
     a.direct_out = L.direct_out;
     a.noisy_out = L.noisy_out;
+    a.rays = L.rays;
+    a.ray_counters = L.ray_counters;
+    a.vis = L.vis;
+    a.pending = L.pending;
     return a;
 }
 
@@ -356,6 +465,11 @@ static cudaError_t launch_typed(const LightingLaunch& L, int stage, cudaStream_t
     switch (stage) {
     case kStageReuse: reuse_kernel<G><<<grid, block, 0, st>>>(f, a, L.keep_candidates); break;
     case kStageShade: shade_kernel<G, R><<<grid, block, 0, st>>>(f, a); break;
+    case kStageSpatial: spatial_prep_kernel<G, R><<<grid, block, 0, st>>>(f, a); break;
+    case kStageCombine: {
+        size_t P = (size_t)f.size[0] * f.size[1];
+        combine_kernel<R><<<(unsigned)((P + 255) / 256), 256, 0, st>>>(f, L.pending, L.vis, L.direct_out, L.noisy_out);
+    } break;
     case 0: pass_kernel<G, R, 0><<<grid, block, 0, st>>>(f, a); break;
     case 1: pass_kernel<G, R, 1><<<grid, block, 0, st>>>(f, a); break;
     case 2: pass_kernel<G, R, 2><<<grid, block, 0, st>>>(f, a); break;

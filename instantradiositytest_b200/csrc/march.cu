@@ -1,0 +1,243 @@
+// march.cu — persistent soft-shadow march over the ray queue.
+//
+// visibility() of sdf.wgsl:61-81 restated as a per-lane state machine whose
+// every iteration issues exactly one scene_distance query: the clearance
+// query at the surface point, the endpoint clearance query for VPL rays, then
+// up to sdf_max_steps march steps.  A lane that finishes its ray refills from
+// the queue on the next iteration (warp-aggregated atomic fetch).
+//
+// scene_distance (sdf.wgsl:42-60) returns the minimum object distance: the
+// walk skips a subtree only when its box bound exceeds the current best, and
+// every object's distance is at least the distance to its BVH leaf box (the
+// leaf box bounds the padded SDF box, which bounds the geometry box the
+// distance is clamped to).  So visiting the same leaves in another order and
+// skipping those whose box bound exceeds the current best yields the same
+// best, the same closest object (ties aside) and the same voxel.  The march
+// visits leaves in the order of a per-frame leaf-order cache: for the grid
+// cell holding the query point, the leaves sorted by their box distance to
+// the cell, stopping at the first whose bound exceeds the best so far.
+// Points outside the grid, or past the cached entries, test every leaf.
+// Per object the arithmetic is object_distance()'s, evaluated on records
+// staged in shared memory.
+#include <cuda_runtime.h>
+
+#include "dev_sdf.cuh"
+#include "kernels.h"
+
+namespace irtd {
+
+enum : uint32_t { kClear = 0, kEndpoint = 1, kMarch = 2 };
+constexpr uint32_t kNone = 0xffffffffu;
+
+__device__ __forceinline__ float object_distance_rec(const DevScene& sc, V3 p, const MObj& o) {
+    DMesh m;
+    m.lo = o.lo;
+    m.hi = o.hi;
+    m.field = o.field;
+    m.grid = o.grid;
+    m.glo = o.glo;
+    m.ghi = o.ghi;
+    m.sphere = o.sphere;
+    return object_distance_rows(sc, p, o.rx, o.ry, o.rz, o.meta.x, m);
+}
+
+struct Grid {
+    const uint4* cells;
+    float ox, oy, oz, ix, iy, iz;
+};
+
+// Leaf `oid` (box of BVH node `leaf`) against the best so far: the walk's
+// pruning test, then the object's distance.
+__device__ __forceinline__ void visit_leaf(const DevScene& sc, const irt_frame& f, const MNode* nodes,
+                                           const MObj* objs, V3 p, uint32_t oid, bool spacing, Dist& r) {
+    const MObj& o = objs[oid];
+    const uint32_t leaf = __float_as_uint(o.meta.w);
+    const float4 a = nodes[leaf].a, b = nodes[leaf].b;
+    V3 delta = vmax(vmax(V3{a.x, a.y, a.z} - p, p - V3{b.x, b.y, b.z}), V3{0.f, 0.f, 0.f});
+    V3 lb = delta * .9998f;
+    float bb = wmax(r.best, 0.f);
+    if (dot(lb, lb) > bb * bb) return;
+    float d = object_distance_rec(sc, p, o);
+    if (d < r.best) {
+        r.best = d;
+        r.voxel = spacing ? o.meta.y : f.sdf[1];
+        r.closest = oid;
+    }
+}
+
+__device__ __forceinline__ Dist scene_distance_cached(const DevScene& sc, const irt_frame& f, const Grid& g,
+                                                      const MNode* nodes, const MObj* objs, V3 p, uint32_t hint,
+                                                      bool spacing) {
+    const uint32_t n = f.counts[3];
+    Dist r{1e20f, f.sdf[1], hint};
+    if (hint < n) {
+        const MObj& o = objs[hint];
+        r.best = object_distance_rec(sc, p, o);
+        if (spacing) r.voxel = o.meta.y;
+    }
+    const float fx = (p.x - g.ox) * g.ix, fy = (p.y - g.oy) * g.iy, fz = (p.z - g.oz) * g.iz;
+    const float G = (float)kGridRes;
+    bool all = !(fx >= 0.f && fy >= 0.f && fz >= 0.f && fx < G && fy < G && fz < G);
+    if (!all) {
+        const uint32_t cell = ((uint32_t)fz * kGridRes + (uint32_t)fy) * kGridRes + (uint32_t)fx;
+        const uint4* c = g.cells + (size_t)cell * (kCellWords / 4);
+        const uint4 ids = __ldg(c);
+        const uint4 l0 = __ldg(c + 1), l1 = __ldg(c + 2);
+        const float4 lb0 = make_float4(__uint_as_float(l0.x), __uint_as_float(l0.y), __uint_as_float(l0.z),
+                                       __uint_as_float(l0.w));
+        const float4 lb1 = make_float4(__uint_as_float(l1.x), __uint_as_float(l1.y), __uint_as_float(l1.z),
+                                       __uint_as_float(l1.w));
+        const float sentinel = __uint_as_float(__ldg(c + 3).x);
+        const uint32_t idw[4] = {ids.x, ids.y, ids.z, ids.w};
+        const float lbs[8] = {lb0.x, lb0.y, lb0.z, lb0.w, lb1.x, lb1.y, lb1.z, lb1.w};
+        bool done = false;
+#pragma unroll
+        for (int j = 0; j < (int)kCellEntries; j++) {
+            if (!done) {
+                const uint32_t oid = (idw[j >> 1] >> ((j & 1) * 16)) & 0xffffu;
+                if (lbs[j] > wmax(r.best, 0.f) || oid == 0xffffu) {
+                    done = true;
+                } else if (oid != hint) {
+                    visit_leaf(sc, f, nodes, objs, p, oid, spacing, r);
+                }
+            }
+        }
+        all = !done && sentinel <= wmax(r.best, 0.f);
+    }
+    if (all) {
+        for (uint32_t oid = 0; oid < n; oid++)
+            if (oid != hint) visit_leaf(sc, f, nodes, objs, p, oid, spacing, r);
+    }
+    return r;
+}
+
+__global__ void __launch_bounds__(128) march_kernel(const __grid_constant__ irt_frame f, const DevScene sc,
+                                                    const float4* __restrict__ march_scene, uint32_t scene_vec4,
+                                                    const Grid grid, const RayRecord* __restrict__ rays,
+                                                    uint32_t* counters, float* __restrict__ vis) {
+    extern __shared__ float4 smem[];
+    for (uint32_t i = threadIdx.x; i < scene_vec4; i += blockDim.x) smem[i] = __ldg(march_scene + i);
+    __syncthreads();
+    const uint32_t n_obj = f.counts[3];
+    const MNode* nodes = reinterpret_cast<const MNode*>(smem);
+    const MObj* objs = reinterpret_cast<const MObj*>(smem + 2 * (2 * n_obj - 1));
+
+    const uint32_t n_rays = *(volatile uint32_t*)&counters[0];
+    const unsigned full = 0xffffffffu;
+    const int lane = threadIdx.x & 31;
+    const float eps = f.sdf[1];
+    const uint32_t max_steps = to_u32(f.sdf[0]);
+
+    bool active = false;
+    bool exhausted = false;  // warp-uniform: the queue has no rays left
+    uint32_t phase = kClear, slot = 0;
+    MarchState m;
+    m.closest = kNone;
+    m.origin = V3{0.f, 0.f, 0.f};  // surface point until the clearance query
+    m.dir = V3{0.f, 0.f, 0.f};     // surface normal until the march begins
+    m.t = m.limit = 0.f;
+    m.result = 1.f;
+    m.previous = 1e20f;
+    m.step = 0;
+    V3 target{0.f, 0.f, 0.f}, endn{0.f, 0.f, 0.f};
+
+    for (;;) {
+        if (!exhausted) {
+            unsigned need = __ballot_sync(full, !active);
+            if (need) {
+                int leader = __ffs(need) - 1;
+                uint32_t cnt = (uint32_t)__popc(need);
+                uint32_t base = 0;
+                if (lane == leader) base = atomicAdd(&counters[1], cnt);
+                base = __shfl_sync(full, base, leader);
+                if (base + cnt >= n_rays) exhausted = true;
+                if (!active) {
+                    uint32_t idx = base + (uint32_t)__popc(need & ((1u << lane) - 1u));
+                    if (idx < n_rays) {
+                        const float4* r = reinterpret_cast<const float4*>(rays + idx);
+                        float4 a = __ldg(r), b = __ldg(r + 1), c = __ldg(r + 2), d = __ldg(r + 3);
+                        m.origin = V3{a.x, a.y, a.z};
+                        slot = __float_as_uint(a.w);
+                        m.dir = V3{b.x, b.y, b.z};
+                        target = V3{c.x, c.y, c.z};
+                        endn = V3{d.x, d.y, d.z};
+                        phase = kClear;
+                        active = true;
+                    }
+                }
+            }
+        }
+        if (!__any_sync(full, active)) break;
+        if (!active) continue;
+
+        V3 q = phase == kClear ? m.origin : (phase == kEndpoint ? target : march_point(m));
+        uint32_t hint = phase == kMarch ? m.closest : kNone;
+        Dist d = scene_distance_cached(sc, f, grid, nodes, objs, q, hint, phase != kMarch);
+
+        float out = -1.f;
+        if (phase == kClear) {
+            m.closest = d.closest;
+            m.origin = m.origin + m.dir * clearance_epsilon(eps, d.voxel);
+            if (dot(endn, endn) > .5f) {
+                phase = kEndpoint;
+            } else {
+                phase = kMarch;
+                out = march_begin(m, target, eps, max_steps);
+            }
+        } else if (phase == kEndpoint) {
+            phase = kMarch;
+            out = march_begin(m, target + endn * clearance_epsilon(eps, d.voxel), eps, max_steps);
+        } else {
+            m.closest = d.closest;
+            out = march_after(m, d.best, eps, f.sdf[2], max_steps);
+        }
+        if (out >= 0.f) {
+            vis[slot] = out;
+            active = false;
+        }
+    }
+}
+
+}  // namespace irtd
+
+uint32_t irt_march_scene_bytes(uint32_t object_count) {
+    return (2 * object_count - 1) * (uint32_t)sizeof(irtd::MNode) + object_count * (uint32_t)sizeof(irtd::MObj);
+}
+
+cudaError_t irt_launch_march(const MarchLaunch& M, cudaStream_t st) {
+    using namespace irtd;
+    const uint32_t smem = irt_march_scene_bytes(M.frame->counts[3]);
+    thread_local int configured_device = -1;
+    thread_local uint32_t configured_smem = 0;
+    thread_local int blocks_per_sm = 0;
+    int device = 0;
+    cudaGetDevice(&device);
+    if (smem != configured_smem || device != configured_device) {
+        configured_device = device;
+        cudaError_t e = cudaFuncSetAttribute(march_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+        if (e != cudaSuccess) return e;
+        e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&blocks_per_sm, march_kernel, 128, smem);
+        if (e != cudaSuccess) return e;
+        if (blocks_per_sm < 1) return cudaErrorInvalidConfiguration;
+        configured_smem = smem;
+    }
+    DevScene sc;
+    sc.objects = M.objects;
+    sc.meshes = M.meshes;
+    sc.nodes = M.nodes;
+    sc.lights = nullptr;
+    sc.atlas = M.atlas;
+    sc.sdf_f16 = M.sdf_f16;
+    sc.error = M.error;
+    Grid g;
+    g.cells = M.cells;
+    g.ox = M.grid_org[0];
+    g.oy = M.grid_org[1];
+    g.oz = M.grid_org[2];
+    g.ix = M.grid_inv[0];
+    g.iy = M.grid_inv[1];
+    g.iz = M.grid_inv[2];
+    march_kernel<<<M.num_sms * blocks_per_sm, 128, smem, st>>>(*M.frame, sc, M.march_scene, smem / 16, g, M.rays,
+                                                                M.ray_counters, M.vis);
+    return cudaGetLastError();
+}

@@ -143,8 +143,11 @@ class Session:
     def set_profiling(self, on=True):
         L.check(lib.irt_session_set_profiling(self.handle, int(on)), self.ctx.handle, "profiling")
 
+    STAGES = ("archive", "reuse", "spatial", "march", "combine", "svgf_temporal", "svgf_variance", "atrous",
+              "history", "total")
+
     def pass_ms(self, frame_index=None):
-        out = (C.c_float * 8)()
+        out = (C.c_float * 10)()
         if frame_index is None:
             L.check(lib.irt_session_pass_ms(self.handle, out), self.ctx.handle, "pass ms")
         else:

@@ -63,7 +63,7 @@ def sync_history(orc: Oracle, drv: FrameDriver, prev_index: int):
 
 
 class Lockstep:
-    def __init__(self, wl: Workload, gbuffer_format=L.GBUFFER_F32, radiance_format=L.RADIANCE_F32, fused=True,
+    def __init__(self, wl: Workload, gbuffer_format=L.GBUFFER_F32, radiance_format=L.RADIANCE_F32, fused=1,
                  precision=0):
         self.wl = wl
         self.drv = FrameDriver(wl, gbuffer_format=gbuffer_format, radiance_format=radiance_format, fused=fused,

@@ -31,15 +31,16 @@ def check(stats, label):
             assert v <= RADIANCE_BAR, f"{label}: {k} = {v}"
 
 
-@pytest.mark.parametrize("fused", [True, False])
-def test_small_room_lockstep_parity(cuda, fused):
-    """256x160 room of 12 meshes, 16 frames, f32 G-buffer and radiance."""
+@pytest.mark.parametrize("schedule", [1, 0])
+def test_small_room_lockstep_parity(cuda, schedule):
+    """256x160 room of 12 meshes, 16 frames, f32 G-buffer and radiance;
+    schedule 1 = ray-queue march, 0 = one kernel per reference entry point."""
     wl = Workload(0)
-    ls = Lockstep(wl, fused=fused)
+    ls = Lockstep(wl, fused=schedule)
     rows = [ls.frame(i) for i in range(16)]
     ls.close()
     stats = summarize(rows)
-    print("lockstep", "fused" if fused else "plain", stats)
+    print("lockstep schedule", schedule, stats)
     check(stats, "lockstep")
 
 
@@ -66,10 +67,11 @@ def test_free_running_images_stay_within_bar(cuda):
     assert r["filtered"] <= 5 * RADIANCE_BAR
 
 
-def test_fused_and_plain_schedules_are_bit_identical(cuda):
+@pytest.mark.parametrize("schedule", [1, 2])
+def test_fused_and_plain_schedules_are_bit_identical(cuda, schedule):
     wl = Workload(0, width=128, height=96)
-    a = FrameDriver(wl, fused=True, keep_candidates=True)
-    b = FrameDriver(wl, fused=False)
+    a = FrameDriver(wl, fused=schedule, keep_candidates=True)
+    b = FrameDriver(wl, fused=0)
     for i in range(6):
         inputs = a.inputs(i)
         a.step(i, inputs=inputs)
