@@ -278,6 +278,27 @@ irt_status irt_session_set_profiling(irt_session* s, int32_t on);
 irt_status irt_session_pass_ms(irt_session* s, float out_ms[10]);
 irt_status irt_session_pass_ms_at(irt_session* s, uint32_t frame_index, float out_ms[10]);
 
+/* SVGF spatial stages (variance bootstrap, then `iterations` a-trous passes)
+ * of one frame for callers that cannot allocate device memory — a frame
+ * thread that must not stall on an allocation, or a host that reserves all
+ * device memory under its own allocator.  No counterpart in the reference
+ * (there the filter's images are Svgf-owned textures).  The caller passes all
+ * inputs (the svgf_temporal radiance and moments a session exposes as
+ * IRT_BUF_TEMPORAL / IRT_BUF_MOMENTS, or its own) and outputs (filtered
+ * image; feedback image of the first pass, may be NULL), in the radiance
+ * format given.  The two ping-pong images between passes live in a fixed
+ * 8 MiB array of this library's device memory that every GPU loading the
+ * library holds until exit; frames above 262144 pixels (512x512) are
+ * rejected.  The first call on each device looks up that array's address,
+ * so it should come before any stream capture.  All calls share the array:
+ * calls that overlap on the GPU race.  No cudaMalloc/cudaFree is called.
+ * `err` (may be NULL) receives a message on failure. */
+irt_status irt_svgf_spatial_noalloc(const irt_frame* frame, const irt_gbuffer* gbuffer,
+                                    int32_t radiance_format, uint32_t iterations,
+                                    const void* temporal_radiance, const float* moments,
+                                    void* filtered_out, void* feedback_out, void* stream,
+                                    char* err, size_t err_len);
+
 /* ---------------------------------------------------------------------------
  * Host logic of src/renderer.rs used to build scene data (C++ equivalents).
  * ------------------------------------------------------------------------- */

@@ -139,6 +139,8 @@ _PROTOS = {
     "irt_session_set_profiling": (I32, [P, I32]),
     "irt_session_pass_ms": (I32, [P, C.POINTER(C.c_float)]),
     "irt_session_pass_ms_at": (I32, [P, U32, C.POINTER(C.c_float)]),
+    "irt_svgf_spatial_noalloc": (I32, [C.POINTER(Frame), C.POINTER(GBuffer), I32, U32, P, P, P, P, P, C.c_char_p,
+                                       C.c_size_t]),
     "irt_is_box_geometry": (I32, [P, U32, P, U32, C.POINTER(C.c_float), C.POINTER(C.c_float)]),
     "irt_field_lipschitz_bound": (C.c_float, [P, U32, C.POINTER(C.c_float)]),
     "irt_mesh_metadata": (I32, [P, U32, P, U32, P, U32, C.POINTER(C.c_float), C.POINTER(C.c_float),
