@@ -52,7 +52,7 @@ sys.path.insert(0, ROOT)
 #   history copy = depth+normal read 20 + write 20                    =  40
 ALG_BYTES = {"reuse": 188, "spatial": 324, "march": 136, "combine": 72, "svgf_temporal": 140, "svgf_variance": 84,
              "atrous": 4 * 68, "history": 40}
-STAGES = ["archive", "reuse", "spatial", "march", "combine", "svgf_temporal", "svgf_variance", "atrous", "history"]
+STAGES = ["prep", "reuse", "spatial", "march", "combine", "svgf_temporal", "svgf_variance", "atrous", "history"]
 KERNELS = ["reuse", "spatial", "march", "combine", "svgf_temporal", "svgf_variance", "atrous"]
 KERNELS_PER_FRAME = 4 + 2 + 4  # reuse, spatial, march, combine, svgf temporal, variance, 4 a-trous
 # Counted FP32 work of the march per oracle work counter (flops): BVH node

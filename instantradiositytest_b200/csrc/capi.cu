@@ -40,14 +40,17 @@ struct irt_scene {
     irt_object* objects = nullptr;
     irt_node* nodes = nullptr;
     irt_light* lights = nullptr;
+    irt_light* lights_prep = nullptr;  // spot direction normalised, cos(angle / 2)
     uint32_t object_cap = 0, light_cap = 0;
     // compact march scene (nodes + object records with their mesh folded in)
     float4* march_scene = nullptr;
     std::vector<float4> march_host;
     // leaf-order cache (rebuilt when the BVH changes)
     uint4* cells = nullptr;
-    std::vector<uint32_t> cells_host;
+    float* corners = nullptr;
+    size_t corner_cap = 0;
     std::vector<irt_node> cached_nodes;
+    std::vector<irt_object> cached_objects;
     float grid_org[3] = {0, 0, 0}, grid_inv[3] = {0, 0, 0};
     uint32_t object_count = 0, light_count = 0;
     uint64_t bytes = 0;
@@ -86,6 +89,10 @@ struct irt_session {
     uint32_t* ray_counters = nullptr;
     float* vis = nullptr;
     float4* pending = nullptr;
+    // per-pixel world positions: [0] this frame, [1] the previous frame's
+    // pixels from the previous depth and previous_inv_vp
+    float4* guide[2] = {nullptr, nullptr};
+    uint32_t guide_frame = 0xffffffffu;
     int num_sms = 0;
     bool ev_ready = false;
     int prof_slot = 0;
@@ -292,9 +299,13 @@ irt_status irt_scene_update(irt_scene* sc, const irt_object* objects, uint32_t o
     }
     if (light_count > sc->light_cap) {
         if (sc->lights) cudaFree(sc->lights);
+        if (sc->lights_prep) cudaFree(sc->lights_prep);
         sc->lights = nullptr;
+        sc->lights_prep = nullptr;
         uint64_t added = 0;
         irt_status s1 = dev_alloc(ctx, &sc->lights, sizeof(irt_light) * light_count, added);
+        if (s1) return s1;
+        s1 = dev_alloc(ctx, &sc->lights_prep, sizeof(irt_light) * light_count, added);
         if (s1) return s1;
         sc->light_cap = light_count;
         sc->bytes += added;
@@ -302,8 +313,10 @@ irt_status irt_scene_update(irt_scene* sc, const irt_object* objects, uint32_t o
     }
     CK(cudaMemcpyAsync(sc->objects, objects, sizeof(irt_object) * object_count, cudaMemcpyHostToDevice, st), "objects");
     CK(cudaMemcpyAsync(sc->nodes, nodes, sizeof(irt_node) * node_count, cudaMemcpyHostToDevice, st), "nodes");
-    if (light_count)
+    if (light_count) {
         CK(cudaMemcpyAsync(sc->lights, lights, sizeof(irt_light) * light_count, cudaMemcpyHostToDevice, st), "lights");
+        CK(irt_launch_prepare_lights(sc->lights, light_count, sc->lights_prep, st), "light preparation");
+    }
     // Compact march scene: the same values, laid out for shared memory.
     const uint32_t mbytes = irt_march_scene_bytes(object_count);
     if (sc->march_host.size() * 16 < mbytes) {
@@ -348,10 +361,11 @@ irt_status irt_scene_update(irt_scene* sc, const irt_object* objects, uint32_t o
                                    m.enclosing_sphere[3]);
     }
     CK(cudaMemcpyAsync(sc->march_scene, sc->march_host.data(), mbytes, cudaMemcpyHostToDevice, st), "march scene");
-    // Leaf-order cache, rebuilt only when the BVH changes (static scenes
-    // build it once).
-    if (sc->cached_nodes.size() != node_count ||
-        std::memcmp(sc->cached_nodes.data(), nodes, sizeof(irt_node) * node_count) != 0) {
+    // Leaf-order cache, rebuilt on the device when the BVH or an object
+    // changes (static scenes build it once).
+    if (sc->cached_nodes.size() != node_count || sc->cached_objects.size() != object_count ||
+        std::memcmp(sc->cached_nodes.data(), nodes, sizeof(irt_node) * node_count) != 0 ||
+        std::memcmp(sc->cached_objects.data(), objects, sizeof(irt_object) * object_count) != 0) {
         const size_t words = (size_t)kGridRes * kGridRes * kGridRes * kCellWords;
         if (!sc->cells) {
             uint64_t added = 0;
@@ -360,10 +374,38 @@ irt_status irt_scene_update(irt_scene* sc, const irt_object* objects, uint32_t o
             sc->bytes += added;
             ctx->in_use += added;
         }
-        sc->cells_host.assign(words, 0u);
-        irt_build_leaf_cache(nodes, object_count, sc->cells_host.data(), sc->grid_org, sc->grid_inv);
-        CK(cudaMemcpyAsync(sc->cells, sc->cells_host.data(), words * 4, cudaMemcpyHostToDevice, st), "leaf cache");
+        const uint32_t R = kGridRes + 1;
+        const size_t corner_floats = (size_t)R * R * R * object_count;
+        if (object_count <= kMaxCornerObjects && sc->corner_cap < corner_floats) {
+            if (sc->corners) cudaFree(sc->corners);
+            sc->corners = nullptr;
+            uint64_t added = 0;
+            irt_status s1 = dev_alloc(ctx, &sc->corners, corner_floats * 4, added);
+            if (s1) return s1;
+            sc->corner_cap = corner_floats;
+            sc->bytes += added;
+            ctx->in_use += added;
+        }
+        LeafCacheLaunch LC{};
+        LC.march_scene = sc->march_scene;
+        LC.n = object_count;
+        LC.atlas = sc->atlas;
+        LC.sdf_f16 = sc->sdf_f16;
+        for (int a = 0; a < 3; a++) {
+            // The grid covers the root box grown by 0.1 % and 1 mm.
+            double ext = (double)nodes[0].hi[a] - (double)nodes[0].lo[a];
+            double lo = (double)nodes[0].lo[a] - 1e-3 * ext - 1e-3;
+            double hi = (double)nodes[0].hi[a] + 1e-3 * ext + 1e-3;
+            LC.grid_org_d[a] = lo;
+            LC.grid_size_d[a] = (hi - lo) / kGridRes;
+            sc->grid_org[a] = (float)lo;
+            sc->grid_inv[a] = (float)(kGridRes / (hi - lo));
+        }
+        LC.corners = object_count <= kMaxCornerObjects ? sc->corners : nullptr;
+        LC.cells = reinterpret_cast<uint32_t*>(sc->cells);
+        CK(irt_launch_leaf_cache(LC, st), "leaf cache");
         sc->cached_nodes.assign(nodes, nodes + node_count);
+        sc->cached_objects.assign(objects, objects + object_count);
     }
     sc->object_count = object_count;
     sc->light_count = light_count;
@@ -379,8 +421,10 @@ void irt_scene_destroy(irt_scene* sc) {
     if (sc->objects) cudaFree(sc->objects);
     if (sc->nodes) cudaFree(sc->nodes);
     if (sc->lights) cudaFree(sc->lights);
+    if (sc->lights_prep) cudaFree(sc->lights_prep);
     if (sc->march_scene) cudaFree(sc->march_scene);
     if (sc->cells) cudaFree(sc->cells);
+    if (sc->corners) cudaFree(sc->corners);
     if (sc->ctx->in_use >= sc->bytes) sc->ctx->in_use -= sc->bytes;
     delete sc;
 }
@@ -400,6 +444,7 @@ uint64_t irt_session_bytes(const irt_session_desc* d) {
     b += P * 16 * 2;   // moments x2
     b += 16;           // error word
     if (d->fused == 1) b += P * (2 * sizeof(RayRecord) + 2 * 4 + 2 * 16) + 16;  // ray queue, vis, pending
+    b += P * 16 * 2;                                                             // position guides
     return b;
 }
 
@@ -473,6 +518,9 @@ irt_status irt_session_create(irt_context* ctx, const irt_session_desc* desc, ir
         if (!st) st = dev_alloc(ctx, &s->vis, P * 2 * 4, used);
         if (!st) st = dev_alloc(ctx, &s->pending, P * 2 * 16, used);
     }
+    for (int k = 0; k < 2; k++) {
+        if (!st) st = dev_alloc(ctx, &s->guide[k], P * 16, used);
+    }
     if (!st && cudaDeviceGetAttribute(&s->num_sms, cudaDevAttrMultiProcessorCount, ctx->device) != cudaSuccess)
         st = IRT_E_CUDA;
     if (st) return fail(st);
@@ -486,7 +534,7 @@ void irt_session_destroy(irt_session* s) {
     void* ptrs[] = {s->dres[0], s->dres[1], s->dres[2], s->ires[0], s->ires[1], s->ires[2], s->archive,
                     s->prev_depth, s->prev_normal, s->direct, s->noisy, s->moments[0], s->moments[1],
                     s->feedback[0], s->feedback[1], s->temporal, s->scratch[0], s->scratch[1], s->filtered, s->error,
-                    s->rays, s->ray_counters, s->vis, s->pending};
+                    s->rays, s->ray_counters, s->vis, s->pending, s->guide[0], s->guide[1]};
     for (void* p : ptrs)
         if (p) cudaFree(p);
     if (s->ev_ready)
@@ -508,6 +556,23 @@ static irt_status check_frame(irt_session* s, const irt_frame* f, const irt_gbuf
         return IRT_E_INVALID;
     }
     return IRT_OK;
+}
+
+// Per-pixel world positions of this frame (current depth, inv_vp) and of the
+// previous frame's pixels (previous depth, previous_inv_vp).
+static cudaError_t compute_guides(irt_session* s, const irt_frame* f, const irt_gbuffer* g, cudaStream_t st) {
+    SvgfLaunch G{};
+    G.frame = f;
+    G.gbuffer = *g;
+    G.old_depth = s->prev_depth;
+    G.old_normal = s->prev_normal;
+    G.out = s->guide[0];
+    cudaError_t e = irt_launch_svgf(G, 3, st);
+    if (e != cudaSuccess) return e;
+    G.out = s->guide[1];
+    e = irt_launch_svgf(G, 4, st);
+    if (e == cudaSuccess) s->guide_frame = f->size[2];
+    return e;
 }
 
 static void mark(irt_session* s, int k, cudaStream_t st) {
@@ -545,6 +610,7 @@ irt_status irt_frame_lighting(irt_session* s, const irt_scene* sc, const irt_fra
     s->prof_slot = (int)(f->size[2] % irt_session::kProfRing);
     s->prof_frame[s->prof_slot] = f->size[2];
     mark(s, 0, st);
+    CK(compute_guides(s, f, g, st), "position guides");
     // VPL archive ring slot frame % (H+1) (src/renderer.rs:1873-1884).
     size_t pool = (size_t)set.vpl_count * sizeof(irt_vpl);
     uint32_t slot = f->size[2] % (set.restir_max_history + 1u);
@@ -556,7 +622,7 @@ irt_status irt_frame_lighting(irt_session* s, const irt_scene* sc, const irt_fra
     L.objects = sc->objects;
     L.meshes = sc->meshes;
     L.nodes = sc->nodes;
-    L.lights = sc->lights;
+    L.lights = sc->lights_prep;
     L.atlas = sc->atlas;
     L.sdf_f16 = sc->sdf_f16;
     L.error = s->error;
@@ -577,6 +643,8 @@ irt_status irt_frame_lighting(irt_session* s, const irt_scene* sc, const irt_fra
     L.ray_counters = s->ray_counters;
     L.vis = s->vis;
     L.pending = s->pending;
+    L.guide = s->guide[0];
+    L.old_guide = s->guide[1];
     if (s->desc.fused == 1) {
         // candidates+temporal -> spatial + resolve set-up (ray queue) ->
         // persistent march -> resolve outputs.
@@ -643,11 +711,15 @@ irt_status irt_frame_svgf(irt_session* s, const irt_frame* f, const irt_gbuffer*
         mark(s, 7, st);
         mark(s, 8, st);
     } else {
+        // Positions for this frame (already there when the lighting ran).
+        if (s->guide_frame != f->size[2]) CK(compute_guides(s, f, g, st), "position guides");
         SvgfLaunch L{};
         L.frame = f;
         L.gbuffer = *g;
         L.old_depth = s->prev_depth;
         L.old_normal = s->prev_normal;
+        L.guide = s->guide[0];
+        L.old_guide = s->guide[1];
         L.radiance_f16 = s->desc.radiance_format == IRT_RADIANCE_F16;
         L.in = s->noisy;
         L.aux = s->feedback[old];

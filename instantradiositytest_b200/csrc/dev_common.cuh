@@ -69,40 +69,60 @@ __device__ __forceinline__ V3 world(float u, float v, float depth, const irt_mat
     return V3{h[0] / h[3], h[1] / h[3], h[2] / h[3]};
 }
 
+// A shading point and the BRDF terms that depend only on it and the camera
+// (computed once per pixel, the same values brdf() would compute per call).
 struct Surface {
     V3 p, n, color;
     float rough, metal;
+    V3 wo;            // normalize(camera - p)
+    float nv, a2, g1v, km;
+    V3 f0;            // mix(vec3(.04), color, metal)
 };
+__device__ __forceinline__ void surface_terms(Surface& s, V3 camera) {
+    s.wo = normalize(camera - s.p);
+    s.nv = wmax(dot(s.n, s.wo), .00001f);
+    float a = s.rough * s.rough;
+    s.a2 = a * a;
+    s.g1v = 2.f * s.nv / (s.nv + sqrtf(s.a2 + (1.f - s.a2) * s.nv * s.nv));
+    s.km = 1.f - s.metal;
+    s.f0 = V3{.04f * s.km + s.color.x * s.metal, .04f * s.km + s.color.y * s.metal, .04f * s.km + s.color.z * s.metal};
+}
 
-// common.wgsl:67-74 (GGX with Smith G1 terms plus Lambert, F0 = mix(.04, c, metal)).
-__device__ __forceinline__ V3 brdf(const Surface& s, V3 wo, V3 wi) {
-    float nv = wmax(dot(s.n, wo), .00001f);
+// common.wgsl:67-74 (GGX with Smith G1 terms plus Lambert, F0 = mix(.04, c, metal))
+// toward wi for the surface's view direction; (1 - vh)^5 by multiplication.
+__device__ __forceinline__ V3 brdf(const Surface& s, V3 wi) {
+    const V3 wo = s.wo;
+    const float nv = s.nv;
     float nl = wmax(dot(s.n, wi), 0.f);
     if (nl <= 0.f) return V3{0.f, 0.f, 0.f};
     V3 h = normalize(wo + wi);
     float nh = wmax(dot(s.n, h), 0.f);
     float vh = wmax(dot(wo, h), 0.f);
-    float a = s.rough * s.rough;
-    float a2 = a * a;
+    const float a2 = s.a2;
     float q = nh * nh * (a2 - 1.f) + 1.f;
     float d = a2 / (kPI * q * q);
-    float g1v = 2.f * nv / (nv + sqrtf(a2 + (1.f - a2) * nv * nv));
     float g1l = 2.f * nl / (nl + sqrtf(a2 + (1.f - a2) * nl * nl));
-    float km = 1.f - s.metal;
-    V3 f0 = V3{.04f * km + s.color.x * s.metal, .04f * km + s.color.y * s.metal, .04f * km + s.color.z * s.metal};
-    float p5 = powf(1.f - vh, 5.f);
+    const float km = s.km;
+    const V3 f0 = s.f0;
+    float x = 1.f - vh;
+    float x2 = x * x;
+    float p5 = x2 * x2 * x;
     V3 fr = V3{f0.x + (1.f - f0.x) * p5, f0.y + (1.f - f0.y) * p5, f0.z + (1.f - f0.z) * p5};
     float den = wmax(4.f * nv * nl, .00001f);
+    float spec = d * s.g1v * g1l / den;
     V3 out;
-    out.x = (1.f - fr.x) * km * s.color.x / kPI + fr.x * d * g1v * g1l / den;
-    out.y = (1.f - fr.y) * km * s.color.y / kPI + fr.y * d * g1v * g1l / den;
-    out.z = (1.f - fr.z) * km * s.color.z / kPI + fr.z * d * g1v * g1l / den;
+    out.x = (1.f - fr.x) * km * s.color.x / kPI + fr.x * spec;
+    out.y = (1.f - fr.y) * km * s.color.y / kPI + fr.y * spec;
+    out.z = (1.f - fr.z) * km * s.color.z / kPI + fr.z * spec;
     return out;
 }
 
 // Light and VPL records as three 16-byte vectors (read-only cache loads).
+// Lights are read from the per-frame prepared copy (prepare_lights_kernel):
+// da holds the normalised spot direction and cos(angle / 2) instead of the
+// raw direction and angle — the two values direct() derives per call.
 struct DLight {
-    float4 ps, da, ct;  // position_strength, direction_angle, color_type
+    float4 ps, da, ct;  // position_strength, (normalised direction, cos half angle), color_type
 };
 struct DVpl {
     float4 pos, nrm, flux;
@@ -116,24 +136,34 @@ __device__ __forceinline__ DVpl load_vpl(const irt_vpl* base, size_t i) {
     return DVpl{__ldg(p), __ldg(p + 1), __ldg(p + 2)};
 }
 
+// Prepared light: the spot direction normalised and cos(angle / 2).
+__device__ __forceinline__ DLight prepare_light(const irt_light& l) {
+    V3 d = normalize(V3{l.direction_angle[0], l.direction_angle[1], l.direction_angle[2]});
+    DLight o;
+    o.ps = make_float4(l.position_strength[0], l.position_strength[1], l.position_strength[2], l.position_strength[3]);
+    o.da = make_float4(d.x, d.y, d.z, cosf(l.direction_angle[3] * .5f));
+    o.ct = make_float4(l.color_type[0], l.color_type[1], l.color_type[2], l.color_type[3]);
+    return o;
+}
+
 // common.wgsl:75-79
-__device__ __forceinline__ V3 direct(const Surface& s, const DLight& l, V3 camera) {
+__device__ __forceinline__ V3 direct(const Surface& s, const DLight& l) {
     V3 delta = xyz(l.ps) - s.p;
     float r2 = wmax(dot(delta, delta), .0001f);
     V3 wi = delta * (1.f / sqrtf(r2));
-    if (l.ct.w > 0.5f && dot(-wi, normalize(xyz(l.da))) < cosf(l.da.w * .5f)) return V3{0.f, 0.f, 0.f};
-    V3 b = brdf(s, normalize(camera - s.p), wi);
+    if (l.ct.w > 0.5f && dot(-wi, xyz(l.da)) < l.da.w) return V3{0.f, 0.f, 0.f};
+    V3 b = brdf(s, wi);
     float nl = wmax(dot(s.n, wi), 0.f);
     float st = l.ps.w;
     return V3{b.x * nl * l.ct.x * st / r2, b.y * nl * l.ct.y * st / r2, b.z * nl * l.ct.z * st / r2};
 }
 
 // common.wgsl:80-83
-__device__ __forceinline__ V3 indirect(const Surface& s, const DVpl& v, V3 camera) {
+__device__ __forceinline__ V3 indirect(const Surface& s, const DVpl& v) {
     V3 delta = xyz(v.pos) - s.p;
     float r2 = wmax(dot(delta, delta), .0025f);
     V3 wi = delta * (1.f / sqrtf(r2));
-    V3 b = brdf(s, normalize(camera - s.p), wi);
+    V3 b = brdf(s, wi);
     float nl = wmax(dot(s.n, wi), 0.f);
     float ne = wmax(dot(xyz(v.nrm), -wi), 0.f);
     float den = 4.f * kPI * r2;

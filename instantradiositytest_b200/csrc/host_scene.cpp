@@ -11,7 +11,6 @@
 #include <vector>
 
 #include "host_math.h"
-#include "kernels.h"
 
 using namespace irt;
 
@@ -330,57 +329,3 @@ void irt_pack_object(const irt_mat4* model, const irt_mat4* previous, uint32_t m
 
 }  // extern "C"
 
-void irt_build_leaf_cache(const irt_node* nodes, uint32_t n, uint32_t* cells, float org[3], float inv[3]) {
-    const uint32_t G = kGridRes;
-    // Leaf boxes per object.
-    std::vector<double> lo(3 * (size_t)n, 0.0), hi(3 * (size_t)n, 0.0);
-    for (uint32_t i = 0; i < 2 * n - 1; i++)
-        if (nodes[i].info[2] == 1u && nodes[i].info[0] < n)
-            for (int a = 0; a < 3; a++) {
-                lo[3 * nodes[i].info[0] + a] = nodes[i].lo[a];
-                hi[3 * nodes[i].info[0] + a] = nodes[i].hi[a];
-            }
-    double glo[3], size[3];
-    for (int a = 0; a < 3; a++) {
-        double ext = (double)nodes[0].hi[a] - (double)nodes[0].lo[a];
-        glo[a] = (double)nodes[0].lo[a] - 1e-3 * ext - 1e-3;
-        double ghi = (double)nodes[0].hi[a] + 1e-3 * ext + 1e-3;
-        size[a] = (ghi - glo[a]) / G;
-        org[a] = (float)glo[a];
-        inv[a] = (float)(1.0 / size[a]);
-    }
-    // A point is filed by float arithmetic; growing each cell by this margin
-    // keeps the point inside the cell box its bounds are computed for.
-    double margin = 1e-4 + 1e-5 * std::max(size[0], std::max(size[1], size[2])) * G;
-#pragma omp parallel for schedule(static)
-    for (int64_t c = 0; c < (int64_t)G * G * G; c++) {
-        uint32_t ix = (uint32_t)(c % G), iy = (uint32_t)((c / G) % G), iz = (uint32_t)(c / (G * G));
-        double clo[3] = {glo[0] + ix * size[0] - margin, glo[1] + iy * size[1] - margin, glo[2] + iz * size[2] - margin};
-        double chi[3] = {glo[0] + (ix + 1) * size[0] + margin, glo[1] + (iy + 1) * size[1] + margin,
-                         glo[2] + (iz + 1) * size[2] + margin};
-        std::vector<std::pair<float, uint32_t>> order(n);
-        for (uint32_t o = 0; o < n; o++) {
-            double s = 0;
-            for (int a = 0; a < 3; a++) {
-                double gap = std::max(0.0, std::max(lo[3 * o + a] - chi[a], clo[a] - hi[3 * o + a]));
-                s += gap * gap;
-            }
-            double d = std::sqrt(s) * 0.9998 * (1.0 - 1e-6);
-            float fd = (float)d;
-            if ((double)fd > d) fd = std::nextafter(fd, 0.f);
-            order[o] = {fd, o};
-        }
-        size_t k = std::min<size_t>(n, kCellEntries);
-        std::partial_sort(order.begin(), order.begin() + std::min<size_t>(n, k + 1), order.end());
-        uint32_t* w = cells + (size_t)c * kCellWords;
-        for (uint32_t j = 0; j < kCellWords; j++) w[j] = 0;
-        for (uint32_t j = 0; j < kCellEntries; j++) {
-            uint32_t id = j < k ? order[j].second : 0xffffu;
-            float lb = j < k ? order[j].first : INFINITY;
-            w[j >> 1] |= (id & 0xffffu) << ((j & 1) * 16);
-            std::memcpy(&w[4 + j], &lb, 4);
-        }
-        float sentinel = n > k ? order[k].first : INFINITY;
-        std::memcpy(&w[12], &sentinel, 4);
-    }
-}

@@ -41,6 +41,8 @@ struct LightingLaunch {
     void* noisy_out;
     int radiance_f16;
     int keep_candidates;
+    const float4* guide;      // world positions of this frame's pixels
+    const float4* old_guide;  // ... of the previous frame's pixels
     // ray-queue resolve (kStageSpatial / march / kStageCombine)
     RayRecord* rays;         // capacity 2 * W * H
     uint32_t* ray_counters;  // [0] rays emitted, [1] rays fetched by the march
@@ -77,12 +79,18 @@ constexpr uint32_t kCellEntries = 8;
 // One cell: 4 x uint4 = ids (8 x u16 in words 0-3), lower bounds (f32 words
 // 4-11), sentinel bound of the first object left out (word 12), pad.
 constexpr uint32_t kCellWords = 16;
-// Builds the leaf-order cache from the BVH nodes (host, OpenMP): grid over
-// the root box, per cell the kCellEntries objects whose leaf boxes are
-// nearest to the cell (distance to the cell grown by a rounding margin,
-// rounded toward zero and scaled by .9998), then the next bound.  `cells`
-// receives kGridRes^3 * kCellWords words.
-void irt_build_leaf_cache(const irt_node* nodes, uint32_t object_count, uint32_t* cells, float org[3], float inv[3]);
+// Leaf-order cache build (leafcache.cu) from the staged march scene.
+struct LeafCacheLaunch {
+    const float4* march_scene;  // nodes + object records on the device
+    uint32_t n;                 // objects
+    cudaTextureObject_t atlas;
+    int sdf_f16;
+    double grid_org_d[3], grid_size_d[3];
+    float* corners;             // (kGridRes+1)^3 * n floats, or null: box bounds only
+    uint32_t* cells;            // kGridRes^3 * kCellWords words
+};
+cudaError_t irt_launch_leaf_cache(const LeafCacheLaunch& L, cudaStream_t st);
+constexpr uint32_t kMaxCornerObjects = 256;  // corner bounds for scenes up to this many objects
 
 struct SvgfLaunch {
     const irt_frame* frame;
@@ -97,7 +105,15 @@ struct SvgfLaunch {
     void* moments_out;       // temporal: current moments
     int step;
     int radiance_f16;
+    const float4* guide;      // per-pixel positions of this frame (or null)
+    const float4* old_guide;  // ... of the previous frame (or null)
 };
+// irt_launch_svgf stages: 0 temporal, 1 variance, 2 a-trous, 3 position guide
+// of this frame (out = float4[W*H]), 4 guide of the previous frame (from
+// old_depth and previous_inv_vp).
 
 cudaError_t irt_launch_lighting(const LightingLaunch& L, int stage, cudaStream_t st);
+// Lights with the spot direction normalised and cos(angle / 2) in
+// direction_angle, the form the lighting kernels read.
+cudaError_t irt_launch_prepare_lights(const irt_light* lights, uint32_t n, irt_light* out, cudaStream_t st);
 cudaError_t irt_launch_svgf(const SvgfLaunch& L, int stage, cudaStream_t st);

@@ -35,6 +35,8 @@ struct LightArgs {
     uint32_t* ray_counters;
     const float* vis;
     float4* pending;
+    const float4* guide;      // world positions of this frame's pixels
+    const float4* old_guide;  // ... of the previous frame's pixels
 };
 
 template <class G>
@@ -51,14 +53,17 @@ struct Px {
     __device__ __forceinline__ float uvy(uint32_t qy) const { return ((float)qy + .5f) / (float)f.size[1]; }
     __device__ __forceinline__ bool valid() const { return a.g.d(id) < 1.f; }
     // lighting.wgsl:30-34
+    // world(pixel_uv(p), depth, inv_vp) of pixel i, precomputed per frame.
+    __device__ __forceinline__ V3 position(size_t i) const { return xyz(__ldg(a.guide + i)); }
     __device__ __forceinline__ Surface surface() const {
         Surface s;
-        s.p = world(uvx(x), uvy(y), a.g.d(id), f.inv_vp);
+        s.p = position(id);
         s.n = normalize(a.g.n(id));
         s.color = a.g.c(id);
         float2 rm = a.g.pm(id);
         s.rough = rm.x;
         s.metal = rm.y;
+        surface_terms(s, camera());
         return s;
     }
     // lighting.wgsl:36-40
@@ -66,7 +71,7 @@ struct Px {
         size_t q = (size_t)qy * f.size[0] + qx;
         float d = a.g.d(q);
         if (d >= 1.f) return false;
-        V3 p = world(uvx(qx), uvy(qy), d, f.inv_vp);
+        V3 p = position(q);
         V3 n = normalize(a.g.n(q));
         return dot(s.n, n) > f.temporal[2] && distance(s.p, p) < f.temporal[1] * wmax(distance(s.p, camera()), 1.f);
     }
@@ -85,7 +90,9 @@ struct Px {
         size_t q = (size_t)qy * f.size[0] + (size_t)qx;
         float d = __ldg(a.prev_depth + q);
         if (d >= 1.f) return false;
-        V3 oldp = world(((float)qx + .5f) / (float)f.size[0], ((float)qy + .5f) / (float)f.size[1], d, f.previous_inv_vp);
+        // world((q + .5) / size, d, previous_inv_vp): the previous frame's
+        // position of q, which is that frame's guide entry.
+        V3 oldp = xyz(__ldg(a.old_guide + q));
         V3 pn = G::decode_normal(__ldg(a.prev_normal + q));
         return dot(s.n, pn) > f.temporal[2] && distance(s.p, oldp) < f.temporal[1] * wmax(distance(s.p, camera()), 1.f);
     }
@@ -118,7 +125,7 @@ struct Px {
             float pdf = 1.f / (float)f.counts[0];
             for (uint32_t i = 0; i < f.restir[0]; i++) {
                 uint32_t lid = min(to_u32(rnd(rng) * (float)f.counts[0]), f.counts[0] - 1u);
-                float target = luminance(direct(s, load_light(a.sc.lights, lid), camera()));
+                float target = luminance(direct(s, load_light(a.sc.lights, lid)));
                 res_add(r, lid, f.size[2], target, pdf, target / pdf, 1u, 0u, rng);
             }
         }
@@ -132,7 +139,7 @@ struct Px {
             float pdf = 1.f / (float)f.counts[1];
             for (uint32_t i = 0; i < f.restir[1]; i++) {
                 uint32_t vid = min(to_u32(rnd(rng) * (float)f.counts[1]), f.counts[1] - 1u);
-                float target = luminance(indirect(s, load_vpl(a.cur, vid), camera()));
+                float target = luminance(indirect(s, load_vpl(a.cur, vid)));
                 res_add(r, vid, f.size[2], target, pdf, target / pdf, 1u, 0u, rng);
             }
         }
@@ -145,7 +152,7 @@ struct Px {
         Res previous = cap(res_load(a.dres[2], (size_t)qy * f.size[0] + (size_t)qx), to_u32(f.rr[2]) * f.restir[0]);
         if (previous.generation == f.size[3] && previous.target > 0.f && previous.id < f.counts[0] &&
             previous.age < to_u32(f.rr[2])) {
-            float target = luminance(direct(s, load_light(a.sc.lights, previous.id), camera()));
+            float target = luminance(direct(s, load_light(a.sc.lights, previous.id)));
             res_add(r, previous.id, previous.source, target, previous.pdf,
                     target * normalization(previous) * (float)previous.count, previous.count, previous.age + 1u, rng);
         }
@@ -156,7 +163,7 @@ struct Px {
         if (!hv) return;
         Res previous = cap(res_load(a.ires[2], (size_t)qy * f.size[0] + (size_t)qx), to_u32(f.rr[2]) * f.restir[1]);
         if (vpl_sample_valid(previous)) {
-            float target = luminance(indirect(s, selected_vpl(previous), camera()));
+            float target = luminance(indirect(s, selected_vpl(previous)));
             res_add(r, previous.id, previous.source, target, previous.pdf,
                     target * normalization(previous) * (float)previous.count, previous.count, previous.age + 1u, rng);
         }
@@ -175,13 +182,13 @@ struct Px {
                 Res previous = res_load(in, (size_t)qy * f.size[0] + (size_t)qx);
                 if (Dom == 0) {
                     if (previous.target > 0.f) {
-                        float target = luminance(direct(s, load_light(a.sc.lights, previous.id), camera()));
+                        float target = luminance(direct(s, load_light(a.sc.lights, previous.id)));
                         res_add(r, previous.id, previous.source, target, previous.pdf,
                                 target * normalization(previous) * (float)previous.count, previous.count, previous.age,
                                 rng);
                     }
                 } else if (vpl_sample_valid(previous)) {
-                    float target = luminance(indirect(s, selected_vpl(previous), camera()));
+                    float target = luminance(indirect(s, selected_vpl(previous)));
                     res_add(r, previous.id, previous.source, target, previous.pdf,
                             target * normalization(previous) * (float)previous.count, previous.count, previous.age, rng);
                 }
@@ -196,7 +203,7 @@ struct Px {
             uint32_t dbg = f.flags[2];
             if (d.target > 0.f && dbg != 2u && dbg < 3u) {
                 DLight l = load_light(a.sc.lights, d.id);
-                V3 value = direct(s, l, camera());
+                V3 value = direct(s, l);
                 if (luminance(value) > 0.f) {
                     float vis = visibility(a.sc, f, s.p, s.n, xyz(l.ps), V3{0.f, 0.f, 0.f});
                     float k = normalization(d);
@@ -218,7 +225,7 @@ struct Px {
         if (ok && dbg != 1u && dbg < 3u) {
             if (vpl_sample_valid(v)) {
                 DVpl smp = selected_vpl(v);
-                V3 value = indirect(s, smp, camera());
+                V3 value = indirect(s, smp);
                 if (luminance(value) > 0.f) {
                     float vis = visibility(a.sc, f, s.p, s.n, xyz(smp.pos), xyz(smp.nrm));
                     float k = normalization(v);
@@ -233,6 +240,17 @@ struct Px {
 template <class R>
 __device__ __forceinline__ void store_noisy(void* out, size_t i, V3 r) {
     R::store(reinterpret_cast<typename R::T*>(out), i, make_float4(wmin(r.x, 65000.f), wmin(r.y, 65000.f), wmin(r.z, 65000.f), 1.f));
+}
+
+// Per-frame prepared lights (normalised spot direction, cos of half angle).
+__global__ void prepare_lights_kernel(const irt_light* lights, uint32_t n, irt_light* out) {
+    uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= n) return;
+    DLight l = prepare_light(lights[i]);
+    float4* o = reinterpret_cast<float4*>(out + i);
+    o[0] = l.ps;
+    o[1] = l.da;
+    o[2] = l.ct;
 }
 
 // ---------------------------------------------------------------- fused kernels
@@ -311,7 +329,7 @@ __global__ void __launch_bounds__(256) spatial_prep_kernel(const __grid_constant
         if (ok) {
             if (rd.target > 0.f && dbg != 2u && dbg < 3u) {
                 DLight l = load_light(a.sc.lights, rd.id);
-                V3 value = direct(s, l, px.camera());
+                V3 value = direct(s, l);
                 if (luminance(value) > 0.f) {
                     float k = normalization(rd);
                     pd = make_float4(value.x * k, value.y * k, value.z * k, 1.f);
@@ -333,7 +351,7 @@ __global__ void __launch_bounds__(256) spatial_prep_kernel(const __grid_constant
         float4 pi = make_float4(0.f, 0.f, 0.f, 0.f);
         if (ok && dbg != 1u && dbg < 3u && px.vpl_sample_valid(ri)) {
             DVpl smp = px.selected_vpl(ri);
-            V3 value = indirect(s, smp, px.camera());
+            V3 value = indirect(s, smp);
             if (luminance(value) > 0.f) {
                 float k = normalization(ri);
                 pi = make_float4(value.x * k, value.y * k, value.z * k, 1.f);
@@ -453,6 +471,8 @@ static LightArgs<G> make_args(const LightingLaunch& L) {
     a.ray_counters = L.ray_counters;
     a.vis = L.vis;
     a.pending = L.pending;
+    a.guide = L.guide;
+    a.old_guide = L.old_guide;
     return a;
 }
 
@@ -484,6 +504,12 @@ static cudaError_t launch_typed(const LightingLaunch& L, int stage, cudaStream_t
 }
 
 }  // namespace irtd
+
+cudaError_t irt_launch_prepare_lights(const irt_light* lights, uint32_t n, irt_light* out, cudaStream_t st) {
+    if (n == 0) return cudaSuccess;
+    irtd::prepare_lights_kernel<<<(n + 127) / 128, 128, 0, st>>>(lights, n, out);
+    return cudaGetLastError();
+}
 
 cudaError_t irt_launch_lighting(const LightingLaunch& L, int stage, cudaStream_t st) {
     using namespace irtd;

@@ -111,7 +111,7 @@ __device__ __forceinline__ Dist scene_distance_cached(const DevScene& sc, const 
     return r;
 }
 
-__global__ void __launch_bounds__(128) march_kernel(const __grid_constant__ irt_frame f, const DevScene sc,
+__global__ void __launch_bounds__(128, 6) march_kernel(const __grid_constant__ irt_frame f, const DevScene sc,
                                                     const float4* __restrict__ march_scene, uint32_t scene_vec4,
                                                     const Grid grid, const RayRecord* __restrict__ rays,
                                                     uint32_t* counters, float* __restrict__ vis) {

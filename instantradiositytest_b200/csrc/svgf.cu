@@ -13,7 +13,22 @@ struct SvgfCtx {
     G g;
     const float* old_depth;
     const typename G::NormalT* old_normal;
+    // Per-pixel world positions of this frame and the previous one
+    // (guide_kernel), or null to evaluate world() per tap; both give the
+    // same values.
+    const float4* guide;
+    const float4* old_guide;
 };
+
+// x^64 as six squarings (the `pow(max(dot, 0), 64)` normal weight).
+__device__ __forceinline__ float pow64(float x) {
+    float y = x * x;
+    y = y * y;
+    y = y * y;
+    y = y * y;
+    y = y * y;
+    return y * y;
+}
 
 struct Guide {
     V3 position, normal, color;
@@ -34,6 +49,7 @@ struct Sv {
     __device__ __forceinline__ float uvy(int32_t y) const { return ((float)(uint32_t)y + .5f) / (float)H; }
     // svgf.wgsl:19
     __device__ __forceinline__ V3 position(int32_t x, int32_t y) const {
+        if (c.guide) return xyz(__ldg(c.guide + idx(x, y)));
         return world(uvx(x), uvy(y), c.g.d(idx(x, y)), f.inv_vp);
     }
     // svgf.wgsl:20-26
@@ -43,7 +59,7 @@ struct Sv {
         float d = __ldg(c.old_depth + q);
         if (d >= 1.f) return false;
         V3 a = position(px, py);
-        V3 b = world(uvx(qx), uvy(qy), d, f.previous_inv_vp);
+        V3 b = c.old_guide ? xyz(__ldg(c.old_guide + q)) : world(uvx(qx), uvy(qy), d, f.previous_inv_vp);
         return distance(a, b) < f.temporal[1] * wmax(distance(a, camera()), 1.f) &&
                dot(c.g.n(idx(px, py)), G::decode_normal(__ldg(c.old_normal + q))) > f.temporal[2];
     }
@@ -67,8 +83,8 @@ struct Sv {
         float dq = c.g.d(q);
         if (dq >= 1.f) return 0.f;
         V3 nq = c.g.n(q);
-        float wn = powf(wmax(dot(a.normal, nq), 0.f), 64.f);
-        V3 wq = world(uvx(qx), uvy(qy), dq, f.inv_vp);
+        float wn = pow64(wmax(dot(a.normal, nq), 0.f));
+        V3 wq = c.guide ? xyz(__ldg(c.guide + q)) : world(uvx(qx), uvy(qy), dq, f.inv_vp);
         float tolerance = wmax(.0001f, a.pixel_scale * stride * .5f);
         float wz = expf(-fabsf(dot(wq - a.position, a.normal)) / tolerance);
         V3 dc = a.color - c.g.c(q);
@@ -193,6 +209,26 @@ __global__ void __launch_bounds__(256) svgf_variance_kernel(const __grid_constan
     R::store(out, i, make_float4(in.x, in.y, in.z, wmin(sigma, 65000.f)));
 }
 
+// World position of every pixel, world(pixel_uv, depth, inv_vp)
+// (common.wgsl:46-47) with its f32 operations rounded one by one, and in w
+// the SVGF pixel scale distance(position, camera) / height (svgf.wgsl:30), or
+// -1 where depth >= 1.  The lighting and SVGF kernels read positions from
+// here instead of recomputing them per neighbour tap.
+// With `previous` set, the same for the previous frame's depth and
+// previous_inv_vp (the positions history_valid / history_ok compare with).
+__global__ void __launch_bounds__(256) guide_kernel(const __grid_constant__ irt_frame f, const float* depth,
+                                                    int previous, float4* out) {
+    size_t i = (size_t)blockIdx.x * blockDim.x + threadIdx.x;
+    const uint32_t W = f.size[0];
+    if (i >= (size_t)W * f.size[1]) return;
+    uint32_t x = (uint32_t)(i % W), y = (uint32_t)(i / W);
+    float d = __ldg(depth + i);
+    V3 p = world(((float)x + .5f) / (float)W, ((float)y + .5f) / (float)f.size[1], d,
+                 previous ? f.previous_inv_vp : f.inv_vp);
+    float s = d < 1.f ? distance(p, V3{f.camera[0], f.camera[1], f.camera[2]}) / (float)f.size[1] : -1.f;
+    out[i] = make_float4(p.x, p.y, p.z, s);
+}
+
 __device__ __forceinline__ float wavelet_kernel(int32_t x) {
     if (x == 0) return 1.f;
     if (x == 1 || x == -1) return 2.f / 3.f;
@@ -260,6 +296,8 @@ static SvgfCtx<G> make_ctx(const SvgfLaunch& L) {
     c.g.motion = reinterpret_cast<decltype(c.g.motion)>(L.gbuffer.motion);
     c.old_depth = L.old_depth;
     c.old_normal = reinterpret_cast<const typename G::NormalT*>(L.old_normal);
+    c.guide = L.guide;
+    c.old_guide = L.old_guide;
     return c;
 }
 
@@ -281,6 +319,12 @@ static cudaError_t svgf_typed(const SvgfLaunch& L, int stage, cudaStream_t st) {
     case 2:
         svgf_atrous_kernel<G, R><<<grid, block, 0, st>>>(f, c, (const T*)L.in, (T*)L.out, (T*)L.out2, L.step);
         break;
+    case 3:
+    case 4: {
+        size_t P = (size_t)f.size[0] * f.size[1];
+        guide_kernel<<<(unsigned)((P + 255) / 256), 256, 0, st>>>(f, stage == 3 ? L.gbuffer.depth : L.old_depth,
+                                                                   stage == 4, (float4*)L.out);
+    } break;
     default: return cudaErrorInvalidValue;
     }
     return cudaGetLastError();
