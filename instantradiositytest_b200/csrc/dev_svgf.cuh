@@ -1,0 +1,111 @@
+// dev_svgf.cuh — shared helpers of the SVGF kernels (svgf.wgsl:18-44, :90):
+// history test, per-pixel guides and the edge-stopping geometry weight.
+#pragma once
+#include "dev_common.cuh"
+#include "kernels.h"
+
+namespace irtd {
+
+template <class G>
+struct SvgfCtx {
+    G g;
+    const float* old_depth;
+    const typename G::NormalT* old_normal;
+    // Per-pixel world positions of this frame and the previous one
+    // (guide_kernel), or null to evaluate world() per tap; both give the
+    // same values.
+    const float4* guide;
+    const float4* old_guide;
+};
+
+// x^64 as six squarings (the `pow(max(dot, 0), 64)` normal weight).
+__device__ __forceinline__ float pow64(float x) {
+    float y = x * x;
+    y = y * y;
+    y = y * y;
+    y = y * y;
+    y = y * y;
+    return y * y;
+}
+
+struct Guide {
+    V3 position, normal, color;
+    float m0, m1, pixel_scale;
+};
+
+template <class G>
+struct Sv {
+    const irt_frame& f;
+    const SvgfCtx<G>& c;
+    int32_t W, H;
+    __device__ __forceinline__ Sv(const irt_frame& fr, const SvgfCtx<G>& cx)
+        : f(fr), c(cx), W((int32_t)fr.size[0]), H((int32_t)fr.size[1]) {}
+    __device__ __forceinline__ size_t idx(int32_t x, int32_t y) const { return (size_t)y * (size_t)W + (size_t)x; }
+    __device__ __forceinline__ bool inside(int32_t x, int32_t y) const { return x >= 0 && y >= 0 && x < W && y < H; }
+    __device__ __forceinline__ V3 camera() const { return V3{f.camera[0], f.camera[1], f.camera[2]}; }
+    __device__ __forceinline__ float uvx(int32_t x) const { return ((float)(uint32_t)x + .5f) / (float)W; }
+    __device__ __forceinline__ float uvy(int32_t y) const { return ((float)(uint32_t)y + .5f) / (float)H; }
+    // svgf.wgsl:19
+    __device__ __forceinline__ V3 position(int32_t x, int32_t y) const {
+        if (c.guide) return xyz(__ldg(c.guide + idx(x, y)));
+        return world(uvx(x), uvy(y), c.g.d(idx(x, y)), f.inv_vp);
+    }
+    // svgf.wgsl:20-26
+    __device__ __forceinline__ bool history_ok(int32_t px, int32_t py, int32_t qx, int32_t qy) const {
+        if (f.flags[0] == 0u || f.flags[1] != f.size[3] || !inside(qx, qy)) return false;
+        size_t q = idx(qx, qy);
+        float d = __ldg(c.old_depth + q);
+        if (d >= 1.f) return false;
+        V3 a = position(px, py);
+        V3 b = c.old_guide ? xyz(__ldg(c.old_guide + q)) : world(uvx(qx), uvy(qy), d, f.previous_inv_vp);
+        return distance(a, b) < f.temporal[1] * wmax(distance(a, camera()), 1.f) &&
+               dot(c.g.n(idx(px, py)), G::decode_normal(__ldg(c.old_normal + q))) > f.temporal[2];
+    }
+    // svgf.wgsl:28-31
+    __device__ __forceinline__ Guide guide(int32_t x, int32_t y) const {
+        Guide a;
+        size_t i = idx(x, y);
+        a.position = position(x, y);
+        a.normal = c.g.n(i);
+        a.color = c.g.c(i);
+        float2 pm = c.g.pm(i);
+        a.m0 = pm.x;
+        a.m1 = pm.y;
+        a.pixel_scale = distance(a.position, camera()) / (float)f.size[1];
+        return a;
+    }
+    // svgf.wgsl:32-44
+    __device__ __forceinline__ float geometry_weight(const Guide& a, int32_t qx, int32_t qy, float stride) const {
+        if (!inside(qx, qy)) return 0.f;
+        size_t q = idx(qx, qy);
+        float dq = c.g.d(q);
+        if (dq >= 1.f) return 0.f;
+        V3 nq = c.g.n(q);
+        float wn = pow64(wmax(dot(a.normal, nq), 0.f));
+        V3 wq = c.guide ? xyz(__ldg(c.guide + q)) : world(uvx(qx), uvy(qy), dq, f.inv_vp);
+        float tolerance = wmax(.0001f, a.pixel_scale * stride * .5f);
+        float wz = expf(-fabsf(dot(wq - a.position, a.normal)) / tolerance);
+        V3 dc = a.color - c.g.c(q);
+        float2 pm = c.g.pm(q);
+        float d0 = a.m0 - pm.x, d1 = a.m1 - pm.y;
+        float wc = expf(-length(dc) * 8.f - sqrtf(d0 * d0 + d1 * d1) * 8.f);
+        return wn * wz * wc;
+    }
+};
+
+template <class G>
+__host__ inline SvgfCtx<G> make_ctx(const SvgfLaunch& L) {
+    SvgfCtx<G> c;
+    c.g.depth = L.gbuffer.depth;
+    c.g.normal = reinterpret_cast<decltype(c.g.normal)>(L.gbuffer.normal);
+    c.g.color = reinterpret_cast<decltype(c.g.color)>(L.gbuffer.color);
+    c.g.params = reinterpret_cast<decltype(c.g.params)>(L.gbuffer.params);
+    c.g.motion = reinterpret_cast<decltype(c.g.motion)>(L.gbuffer.motion);
+    c.old_depth = L.old_depth;
+    c.old_normal = reinterpret_cast<const typename G::NormalT*>(L.old_normal);
+    c.guide = L.guide;
+    c.old_guide = L.old_guide;
+    return c;
+}
+
+}  // namespace irtd

@@ -117,3 +117,5 @@ cudaError_t irt_launch_lighting(const LightingLaunch& L, int stage, cudaStream_t
 // direction_angle, the form the lighting kernels read.
 cudaError_t irt_launch_prepare_lights(const irt_light* lights, uint32_t n, irt_light* out, cudaStream_t st);
 cudaError_t irt_launch_svgf(const SvgfLaunch& L, int stage, cudaStream_t st);
+// Stages 1 (variance) and 2 (a-trous), the fast-math SVGF passes.
+cudaError_t irt_launch_svgf_spatial(const SvgfLaunch& L, int stage, cudaStream_t st);

@@ -1,0 +1,139 @@
+// svgf_spatial.cu — svgf_variance (svgf.wgsl:77-89) and svgf_atrous
+// (svgf.wgsl:90-110) as sm_100a CUDA, built with fast math (approximate
+// exp, division and square root): these passes only weight and average
+// radiance, and their inputs (positions, history length) come exactly from
+// the guide and temporal kernels.  One thread per pixel in 32x8 blocks;
+// neighbour taps read through L1 (2-D block locality).
+#include <cuda_runtime.h>
+
+#include "dev_svgf.cuh"
+#include "kernels.h"
+
+namespace irtd {
+
+// svgf.wgsl:77-89
+template <class G, class R>
+__global__ void __launch_bounds__(256) svgf_variance_kernel(const __grid_constant__ irt_frame f, const __grid_constant__ SvgfCtx<G> c,
+                                                            const typename R::T* input, const float4* moments,
+                                                            typename R::T* out) {
+    int32_t x = blockIdx.x * blockDim.x + threadIdx.x;
+    int32_t y = blockIdx.y * blockDim.y + threadIdx.y;
+    Sv<G> sv(f, c);
+    if (x >= sv.W || y >= sv.H) return;
+    size_t i = sv.idx(x, y);
+    float4 in = R::load(input, i);
+    float age = moments[i].z;
+    float sigma = in.w;
+    if (age < 4.f && c.g.d(i) < 1.f) {
+        float s0 = 0.f, s1 = 0.f, total = 0.f;
+        Guide a = sv.guide(x, y);
+        for (int32_t yy = -3; yy <= 3; yy++)
+            for (int32_t xx = -3; xx <= 3; xx++) {
+                int32_t qx = x + xx, qy = y + yy;
+                float w = sv.geometry_weight(a, qx, qy, 1.f);
+                if (w <= 0.f) continue;
+                float4 m = moments[sv.idx(qx, qy)];
+                s0 += m.x * w;
+                s1 += m.y * w;
+                total += w;
+            }
+        float dn = wmax(total, .00001f);
+        s0 /= dn;
+        s1 /= dn;
+        sigma = sqrtf(wmax(s1 - s0 * s0, 0.f) * 4.f / wmax(age, 1.f));
+    }
+    R::store(out, i, make_float4(in.x, in.y, in.z, wmin(sigma, 65000.f)));
+}
+
+__device__ __forceinline__ float wavelet_kernel(int32_t x) {
+    if (x == 0) return 1.f;
+    if (x == 1 || x == -1) return 2.f / 3.f;
+    return 1.f / 6.f;
+}
+
+// svgf.wgsl:91-110; `out2` (optional) receives a second copy of the result.
+template <class G, class R>
+__global__ void __launch_bounds__(256) svgf_atrous_kernel(const __grid_constant__ irt_frame f, const __grid_constant__ SvgfCtx<G> c,
+                                                          const typename R::T* input, typename R::T* out,
+                                                          typename R::T* out2, int32_t step) {
+    int32_t x = blockIdx.x * blockDim.x + threadIdx.x;
+    int32_t y = blockIdx.y * blockDim.y + threadIdx.y;
+    Sv<G> sv(f, c);
+    if (x >= sv.W || y >= sv.H) return;
+    size_t i = sv.idx(x, y);
+    float4 c4 = R::load(input, i);
+    if (c.g.d(i) >= 1.f) {
+        R::store(out, i, c4);
+        if (out2) R::store(out2, i, c4);
+        return;
+    }
+    float variance = 0.f, guide_weight = 0.f;
+    Guide a = sv.guide(x, y);
+#pragma unroll
+    for (int32_t yy = -1; yy <= 1; yy++)
+#pragma unroll
+        for (int32_t xx = -1; xx <= 1; xx++) {
+            int32_t qx = min(max(x + xx, 0), sv.W - 1);
+            int32_t qy = min(max(y + yy, 0), sv.H - 1);
+            float w = (xx == 0 ? 2.f : 1.f) * (yy == 0 ? 2.f : 1.f);
+            float s = R::load(input, sv.idx(qx, qy)).w;
+            variance += s * s * w;
+            guide_weight += w;
+        }
+    float phi = 4.f * sqrtf(variance / wmax(guide_weight, .00001f)) + .0001f;
+    V3 sum = V3{0.f, 0.f, 0.f};
+    float total = 0.f, v = 0.f;
+    float lc = luminance(V3{c4.x, c4.y, c4.z});
+    for (int32_t yy = -2; yy <= 2; yy++)
+        for (int32_t xx = -2; xx <= 2; xx++) {
+            int32_t qx = x + xx * step, qy = y + yy * step;
+            float geom = sv.geometry_weight(a, qx, qy, (float)step);
+            if (geom <= 0.f) continue;
+            float4 smp = R::load(input, sv.idx(qx, qy));
+            float w = wavelet_kernel(xx) * wavelet_kernel(yy) * geom *
+                      expf(-fabsf(luminance(V3{smp.x, smp.y, smp.z}) - lc) / phi);
+            sum = sum + V3{smp.x, smp.y, smp.z} * w;
+            v += smp.w * smp.w * w * w;
+            total += w;
+        }
+    float dn = wmax(total, .00001f);
+    float4 o = make_float4(sum.x / dn, sum.y / dn, sum.z / dn, wmin(sqrtf(v) / dn, 65000.f));
+    R::store(out, i, o);
+    if (out2) R::store(out2, i, o);
+}
+
+template <class G, class R>
+static cudaError_t spatial_typed(const SvgfLaunch& L, int stage, cudaStream_t st) {
+    SvgfCtx<G> c = make_ctx<G>(L);
+    const irt_frame& f = *L.frame;
+    typedef typename R::T T;
+    dim3 block(32, 8);
+    dim3 grid((f.size[0] + 31) / 32, (f.size[1] + 7) / 8);
+    if (stage == 1)
+        svgf_variance_kernel<G, R><<<grid, block, 0, st>>>(f, c, (const T*)L.in, (const float4*)L.moments_in, (T*)L.out);
+    else if (stage == 2)
+        svgf_atrous_kernel<G, R><<<grid, block, 0, st>>>(f, c, (const T*)L.in, (T*)L.out, (T*)L.out2, L.step);
+    else
+        return cudaErrorInvalidValue;
+    return cudaGetLastError();
+}
+
+}  // namespace irtd
+
+cudaError_t irt_launch_svgf_spatial(const SvgfLaunch& L, int stage, cudaStream_t st) {
+    using namespace irtd;
+    if (L.radiance_f16) {
+        switch (L.gbuffer.format) {
+        case IRT_GBUFFER_F32: return spatial_typed<GbF32, RadF16>(L, stage, st);
+        case IRT_GBUFFER_F16: return spatial_typed<GbF16, RadF16>(L, stage, st);
+        case IRT_GBUFFER_PACKED: return spatial_typed<GbPacked, RadF16>(L, stage, st);
+        }
+    } else {
+        switch (L.gbuffer.format) {
+        case IRT_GBUFFER_F32: return spatial_typed<GbF32, RadF32>(L, stage, st);
+        case IRT_GBUFFER_F16: return spatial_typed<GbF16, RadF32>(L, stage, st);
+        case IRT_GBUFFER_PACKED: return spatial_typed<GbPacked, RadF32>(L, stage, st);
+        }
+    }
+    return cudaErrorInvalidValue;
+}
