@@ -208,6 +208,8 @@ typedef struct irt_session_desc {
                                  and spatial+resolve with the march inline per pixel; 0 = one kernel
                                  per reference entry point.  All three give identical results. */
     int32_t keep_candidates;  /* 1 = also write the candidates reservoirs [0] (parity/debug) */
+    int32_t exact_march;      /* schedule 1: 1 = IEEE division and square root in the march
+                                 (bit-identical to schedules 0 and 2); 0 = approximate (default) */
 } irt_session_desc;
 
 /* Allocates the session's persistent history (reservoirs, VPL archive, SVGF

@@ -71,6 +71,7 @@ class SessionDesc(C.Structure):
     _fields_ = [
         ("settings", Settings), ("gbuffer_format", C.c_int32), ("radiance_format", C.c_int32),
         ("moments_format", C.c_int32), ("fused", C.c_int32), ("keep_candidates", C.c_int32),
+        ("exact_march", C.c_int32),
     ]
 
 

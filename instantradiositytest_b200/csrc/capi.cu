@@ -671,6 +671,7 @@ irt_status irt_frame_lighting(irt_session* s, const irt_scene* sc, const irt_fra
         M.ray_counters = s->ray_counters;
         M.vis = s->vis;
         M.num_sms = s->num_sms;
+        M.fast = s->desc.exact_march ? 0 : 1;
         CK(irt_launch_march(M, st), "march kernel");
         mark(s, 4, st);
         CK(irt_launch_lighting(L, kStageCombine, st), "combine kernel");

@@ -68,6 +68,7 @@ struct MarchLaunch {
     uint32_t* ray_counters;
     float* vis;
     int num_sms;
+    int fast;  // 1: approximate division / square root build (march_fast.cu)
 };
 cudaError_t irt_launch_march(const MarchLaunch& M, cudaStream_t st);
 // Bytes of the compact march scene of `object_count` objects: 2N-1 nodes of

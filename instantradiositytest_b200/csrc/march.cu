@@ -19,12 +19,25 @@
 // Points outside the grid, or past the cached entries, test every leaf.
 // Per object the arithmetic is object_distance()'s, evaluated on records
 // staged in shared memory.
+//
+// This file is built twice: as is (IEEE division and square root, the
+// arithmetic of the per-pixel visibility()), and through march_fast.cu with
+// approximate division and square root for the default fast march.
 #include <cuda_runtime.h>
 
 #include "dev_sdf.cuh"
 #include "kernels.h"
 
+#ifndef IRT_MARCH_FAST
+#define IRT_MARCH_FAST 0
+#endif
+
 namespace irtd {
+#if IRT_MARCH_FAST
+namespace fast {
+#else
+namespace exact {
+#endif
 
 enum : uint32_t { kClear = 0, kEndpoint = 1, kMarch = 2 };
 constexpr uint32_t kNone = 0xffffffffu;
@@ -81,26 +94,17 @@ __device__ __forceinline__ Dist scene_distance_cached(const DevScene& sc, const 
     if (!all) {
         const uint32_t cell = ((uint32_t)fz * kGridRes + (uint32_t)fy) * kGridRes + (uint32_t)fx;
         const uint4* c = g.cells + (size_t)cell * (kCellWords / 4);
-        const uint4 ids = __ldg(c);
-        const uint4 l0 = __ldg(c + 1), l1 = __ldg(c + 2);
-        const float4 lb0 = make_float4(__uint_as_float(l0.x), __uint_as_float(l0.y), __uint_as_float(l0.z),
-                                       __uint_as_float(l0.w));
-        const float4 lb1 = make_float4(__uint_as_float(l1.x), __uint_as_float(l1.y), __uint_as_float(l1.z),
-                                       __uint_as_float(l1.w));
-        const float sentinel = __uint_as_float(__ldg(c + 3).x);
-        const uint32_t idw[4] = {ids.x, ids.y, ids.z, ids.w};
-        const float lbs[8] = {lb0.x, lb0.y, lb0.z, lb0.w, lb1.x, lb1.y, lb1.z, lb1.w};
+        const uint32_t* cw = reinterpret_cast<const uint32_t*>(c);
+        const float sentinel = __uint_as_float(__ldg(cw + 12));
         bool done = false;
-#pragma unroll
+#pragma unroll 1
         for (int j = 0; j < (int)kCellEntries; j++) {
-            if (!done) {
-                const uint32_t oid = (idw[j >> 1] >> ((j & 1) * 16)) & 0xffffu;
-                if (lbs[j] > wmax(r.best, 0.f) || oid == 0xffffu) {
-                    done = true;
-                } else if (oid != hint) {
-                    visit_leaf(sc, f, nodes, objs, p, oid, spacing, r);
-                }
+            const uint32_t oid = (__ldg(cw + (j >> 1)) >> ((j & 1) * 16)) & 0xffffu;
+            if (__uint_as_float(__ldg(cw + 4 + j)) > wmax(r.best, 0.f) || oid == 0xffffu) {
+                done = true;
+                break;
             }
+            if (oid != hint) visit_leaf(sc, f, nodes, objs, p, oid, spacing, r);
         }
         all = !done && sentinel <= wmax(r.best, 0.f);
     }
@@ -198,14 +202,20 @@ __global__ void __launch_bounds__(128, 6) march_kernel(const __grid_constant__ i
     }
 }
 
+}  // namespace fast / exact
 }  // namespace irtd
 
-uint32_t irt_march_scene_bytes(uint32_t object_count) {
-    return (2 * object_count - 1) * (uint32_t)sizeof(irtd::MNode) + object_count * (uint32_t)sizeof(irtd::MObj);
-}
+#if IRT_MARCH_FAST
+#define IRT_MARCH_NS irtd::fast
+#define IRT_MARCH_LAUNCH irt_launch_march_fast
+#else
+#define IRT_MARCH_NS irtd::exact
+#define IRT_MARCH_LAUNCH irt_launch_march_exact
+#endif
 
-cudaError_t irt_launch_march(const MarchLaunch& M, cudaStream_t st) {
+cudaError_t IRT_MARCH_LAUNCH(const MarchLaunch& M, cudaStream_t st) {
     using namespace irtd;
+    using namespace IRT_MARCH_NS;
     const uint32_t smem = irt_march_scene_bytes(M.frame->counts[3]);
     thread_local int configured_device = -1;
     thread_local uint32_t configured_smem = 0;
@@ -241,3 +251,15 @@ cudaError_t irt_launch_march(const MarchLaunch& M, cudaStream_t st) {
                                                                 M.ray_counters, M.vis);
     return cudaGetLastError();
 }
+
+#if !IRT_MARCH_FAST
+uint32_t irt_march_scene_bytes(uint32_t object_count) {
+    return (2 * object_count - 1) * (uint32_t)sizeof(irtd::MNode) + object_count * (uint32_t)sizeof(irtd::MObj);
+}
+
+cudaError_t irt_launch_march_fast(const MarchLaunch& M, cudaStream_t st);
+
+cudaError_t irt_launch_march(const MarchLaunch& M, cudaStream_t st) {
+    return M.fast ? irt_launch_march_fast(M, st) : irt_launch_march_exact(M, st);
+}
+#endif

@@ -81,8 +81,9 @@ class Scene:
 
 
 def session_desc(settings: L.Settings, gbuffer_format=L.GBUFFER_F32, radiance_format=L.RADIANCE_F32, fused=True,
-                 keep_candidates=False) -> L.SessionDesc:
-    return L.SessionDesc(settings, gbuffer_format, radiance_format, L.MOMENTS_F32, int(fused), int(keep_candidates))
+                 keep_candidates=False, exact_march=False) -> L.SessionDesc:
+    return L.SessionDesc(settings, gbuffer_format, radiance_format, L.MOMENTS_F32, int(fused), int(keep_candidates),
+                         int(exact_march))
 
 
 class Session:
@@ -184,14 +185,15 @@ class FrameDriver:
     them and calls the C-ABI (the role of Renderer::encode)."""
 
     def __init__(self, wl: Workload, ctx: Context | None = None, gbuffer_format=L.GBUFFER_F32,
-                 radiance_format=L.RADIANCE_F32, fused=True, keep_candidates=False, gpu_gbuffer=False):
+                 radiance_format=L.RADIANCE_F32, fused=True, keep_candidates=False, gpu_gbuffer=False,
+                 exact_march=False):
         self.wl = wl
         self.ctx = ctx or Context()
         self.own_ctx = ctx is None
         self.fmt = gbuffer_format
         self.scene = Scene(self.ctx, wl.meshes, wl.atlas, wl.sdf_format)
         self.session = Session(self.ctx, session_desc(wl.settings, gbuffer_format, radiance_format, fused,
-                                                      keep_candidates))
+                                                      keep_candidates, exact_march))
         self.gpu_gbuffer = gpu_gbuffer
         self.prev_vpls = None
         self.last = None
