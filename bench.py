@@ -66,7 +66,7 @@ FP32_PEAK_TFLOPS = 148 * 128 * 2 * 1.965e9 / 1e12
 def parse():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
-    ap.add_argument("--steps", type=int, default=24)
+    ap.add_argument("--steps", type=int, default=120)
     ap.add_argument("--warmup", type=int, default=8)
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
     ap.add_argument("--config", type=int, default=1)
@@ -113,56 +113,99 @@ def describe(spec, frames, schedule):
 
 
 class Clocks:
-    """nvidia-smi samples (SM clock, reasons) during the timed region."""
+    """SM clock and clock-event reasons sampled during the timed region.
 
-    Q = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+    NVML (the library nvidia-smi reads) is polled from a thread every 20 ms,
+    each sample stamped on the host clock, so only the samples taken inside
+    the timed span are kept.  Falls back to `nvidia-smi --query-gpu ... -lms`
+    when NVML cannot be loaded.  Nothing here changes a GPU setting."""
+
+    Q = ("timestamp,index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
          "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
          "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+    NAMES = ("hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap")
 
-    def __init__(self, index):
-        self.index = index
+    def __init__(self, device):
+        self.device = device
+        self.samples = []  # (host time, sm MHz, max MHz, reasons)
+        self.stop_flag = threading.Event()
+        self.thread = None
         self.proc = None
-        self.lines = []
+
+    def _nvml_handle(self):
+        import pynvml as N
+        N.nvmlInit()
+        try:
+            uuid = str(torch.cuda.get_device_properties(self.device).uuid)
+            return N, N.nvmlDeviceGetHandleByUUID(uuid if uuid.startswith("GPU-") else "GPU-" + uuid)
+        except Exception:
+            return N, N.nvmlDeviceGetHandleByIndex(self.device)
 
     def start(self):
         try:
-            self.proc = subprocess.Popen(["nvidia-smi", f"--id={self.index}", f"--query-gpu={self.Q}",
-                                          "--format=csv,noheader,nounits", "-lms", "200"],
+            N, h = self._nvml_handle()
+            bits = {"hw_slowdown": N.nvmlClocksEventReasonHwSlowdown,
+                    "hw_thermal_slowdown": N.nvmlClocksEventReasonHwThermalSlowdown,
+                    "sw_thermal_slowdown": N.nvmlClocksEventReasonSwThermalSlowdown,
+                    "sw_power_cap": N.nvmlClocksEventReasonSwPowerCap}
+            mx = float(N.nvmlDeviceGetMaxClockInfo(h, N.NVML_CLOCK_SM))
+
+            def poll():
+                while not self.stop_flag.is_set():
+                    try:
+                        sm = float(N.nvmlDeviceGetClockInfo(h, N.NVML_CLOCK_SM))
+                        r = N.nvmlDeviceGetCurrentClocksEventReasons(h)
+                        self.samples.append((time.time(), sm, mx, {k for k, b in bits.items() if r & b}))
+                    except Exception:
+                        pass
+                    self.stop_flag.wait(0.02)
+
+            self.thread = threading.Thread(target=poll, daemon=True)
+            self.thread.start()
+        except Exception:
+            self._start_smi()
+
+    def _start_smi(self):
+        try:
+            self.proc = subprocess.Popen(["nvidia-smi", f"--id={self.device}", f"--query-gpu={self.Q}",
+                                          "--format=csv,noheader,nounits", "-lms", "50"],
                                          stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True)
-            self.t = threading.Thread(target=self._read, daemon=True)
-            self.t.start()
+
+            def read():
+                for line in self.proc.stdout:
+                    parts = [p.strip() for p in line.split(",")]
+                    if len(parts) < 10:
+                        continue
+                    try:
+                        t = datetime.datetime.strptime(parts[0], "%Y/%m/%d %H:%M:%S.%f").timestamp()
+                        sm, mx = float(parts[2]), float(parts[3])
+                    except ValueError:
+                        continue
+                    self.samples.append((t, sm, mx, {n for n, v in zip(self.NAMES, parts[6:10])
+                                                     if v.lower().startswith("active")}))
+
+            self.thread = threading.Thread(target=read, daemon=True)
+            self.thread.start()
         except OSError:
             self.proc = None
 
-    def _read(self):
-        for line in self.proc.stdout:
-            self.lines.append(line.strip())
-
-    def stop(self):
-        if not self.proc:
-            return None
-        self.proc.terminate()
-        try:
-            self.proc.wait(timeout=5)
-        except subprocess.TimeoutExpired:
-            self.proc.kill()
-        sm, mx, reasons = [], 0.0, set()
-        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
-        for ln in self.lines:
-            parts = [p.strip() for p in ln.split(",")]
-            if len(parts) < 9:
-                continue
+    def stop(self, t0, t1):
+        self.stop_flag.set()
+        if self.proc:
+            self.proc.terminate()
             try:
-                sm.append(float(parts[1]))
-                mx = max(mx, float(parts[2]))
-            except ValueError:
-                continue
-            for n, v in zip(names, parts[5:9]):
-                if v.lower().startswith("active"):
-                    reasons.add(n)
-        if not sm:
+                self.proc.wait(timeout=5)
+            except subprocess.TimeoutExpired:
+                self.proc.kill()
+        if self.thread:
+            self.thread.join(timeout=5)
+        inside = [s for s in self.samples if t0 <= s[0] <= t1]
+        if not inside:
             return None
-        return {"sm_mhz": statistics.median(sm), "sm_max_mhz": mx, "reasons": sorted(reasons), "samples": len(sm)}
+        reasons = set().union(*(s[3] for s in inside))
+        return {"sm_mhz": statistics.median(s[1] for s in inside), "sm_max_mhz": max(s[2] for s in inside),
+                "reasons": sorted(reasons), "samples": len(inside),
+                "source": "nvml" if self.proc is None else "nvidia-smi"}
 
 
 def measured_peak():
@@ -317,26 +360,28 @@ def ours(args):
         prev = vpls[i - 1] if i > 0 else zero_vpls
         sess.render(scene, f, gbufs[i][1], C.c_void_p(vpls[i].data_ptr()), C.c_void_p(prev.data_ptr()), sh)
 
+    clocks = Clocks(dev)
+    clocks.start()  # sampling runs from the warm-up on; samples are kept for the timed span
     for i in range(Wm):
         render(i)
     torch.cuda.synchronize()
     if dist:
         dist.barrier()
     sess.set_profiling(True)
-    clocks = Clocks(dev)
-    clocks.start()
     torch.cuda.synchronize()
     if dist:
         dist.barrier()
     e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    t_start = time.time()
     e0.record(stream)
     for i in range(Wm, Wm + K):
         render(i)
     e1.record(stream)
     torch.cuda.synchronize()
+    t_end = time.time()
     if dist:
         dist.barrier()
-    clk = clocks.stop()
+    clk = clocks.stop(t_start, t_end)
     ms = e0.elapsed_time(e1)
     ring0 = max(Wm, Wm + K - 128)  # the session keeps events of the last 128 frames
     stage = np.array([sess.pass_ms(i) for i in range(ring0, Wm + K)])  # [K, 10]
