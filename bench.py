@@ -34,27 +34,58 @@ import numpy as np
 ROOT = os.path.dirname(os.path.abspath(__file__))
 sys.path.insert(0, ROOT)
 
-# Algorithmic bytes per pixel and kernel for the f32 G-buffer / f32 radiance
-# schedule (every surface counted once per kernel that touches it; neighbour
-# taps are cache traffic, not HBM):
-#   reuse   = G-buffer 44 (depth 4, normal 12, colour 12, params 8, motion 8)
-#             + previous depth/normal 16 + history reservoirs D/I 64
-#             + reservoirs [1] D/I written 64                         = 188
-#   spatial = G-buffer 36 (no motion) + reservoirs [1] 64 + [2] written 64
-#             + contributions 32 + 2 ray records 128 written          = 324
+# Algorithmic bytes per pixel and kernel (every surface counted once per
+# kernel that touches it; neighbour taps are cache traffic, not HBM).  With
+# G = G-buffer bytes read (depth, normal, colour, params, motion), Gs = G
+# without motion, prev = previous depth + normal, r = radiance texel,
+# m = moments texel, reservoirs 32 B, ray records 64 B:
+#   reuse   = G + prev + history reservoirs D/I 64 + reservoirs [1] written 64
+#   spatial = Gs + reservoirs [1] 64 + [2] written 64 + contributions 32
+#             + 2 ray records 128 written
 #   march   = 2 ray records 128 read + 2 visibilities 8 written       = 136
-#   combine = contributions 32 + visibilities 8 + direct 16 + noisy 16 = 72
-#   svgf_temporal = noisy 16 + G-buffer 44 + feedback 16 + moments 16
-#             + previous depth/normal 16 + temporal 16 + moments 16   = 140
-#   svgf_variance = temporal 16 + moments 16 + G-buffer guides 36
-#             + output 16                                             =  84
-#   atrous  = input 16 + guides 36 + output 16                        =  68 (x4)
-#   history copy = depth+normal read 20 + write 20                    =  40
-ALG_BYTES = {"reuse": 188, "spatial": 324, "march": 136, "combine": 72, "svgf_temporal": 140, "svgf_variance": 84,
-             "atrous": 4 * 68, "history": 40}
+#   combine = contributions 32 + visibilities 8 + direct 16 + noisy r
+#   svgf_temporal = noisy r + G + feedback r + moments m + prev + temporal r + moments m
+#   svgf_variance = temporal r + moments m + Gs + output r
+#   atrous  = 4 x (input r + Gs + output r)
+#   history = previous depth/normal planes read + written
+# f32 storage: G = 4+12+12+8+8 = 44 -> 188, 324, 136, 72, 140, 84, 4x68, 40.
+# Mixed precision (packed G-buffer, f16 radiance and moments):
+#   G = 4+4+4+4+4 = 20 -> 156, 304, 136, 64, 68, 40, 4x32, 16.
+GBUFFER_READ = {0: (4, 12, 12, 8, 8), 1: (4, 6, 6, 4, 4), 2: (4, 4, 4, 4, 4)}
+NORMAL_STORED = {0: 16, 1: 8, 2: 4}
+
+
+def alg_bytes(gfmt, rfmt, mfmt):
+    d, n, c, pm, mv = GBUFFER_READ[gfmt]
+    G = d + n + c + pm + mv
+    Gs = G - mv
+    prev = d + n
+    r = 8 if rfmt else 16
+    m = 8 if mfmt else 16
+    return {"reuse": G + prev + 128, "spatial": Gs + 288, "march": 136, "combine": 56 + r,
+            "svgf_temporal": 3 * r + G + 2 * m + prev, "svgf_variance": 2 * r + m + Gs, "atrous": 4 * (2 * r + Gs),
+            "history": 2 * (d + NORMAL_STORED[gfmt])}
+
+
+ALG_BYTES = alg_bytes(0, 0, 0)
+
+
+def storage_of(config):
+    """(G-buffer, radiance, moments) formats of a workload preset: the
+    mixed-precision preset stores the packed G-buffer and f16 histories."""
+    if config == 2:
+        return 2, 1, 1, "packed G-buffer (oct normals, RGBA8 albedo, f16 params/motion), f16 SDF with per-mesh " \
+                        "scale, f16 radiance, f16 (mean, deviation) moments; f32 reservoirs and accumulation"
+    return 0, 0, 0, "f32 G-buffer, f32 SDF, f32 radiance, f32 moments"
+
+
 STAGES = ["prep", "reuse", "spatial", "march", "combine", "svgf_temporal", "svgf_variance", "atrous", "history"]
 KERNELS = ["reuse", "spatial", "march", "combine", "svgf_temporal", "svgf_variance", "atrous"]
-KERNELS_PER_FRAME = 4 + 2 + 4  # reuse, spatial, march, combine, svgf temporal, variance, 4 a-trous
+# Kernels launched per frame: light preparation (scene update), 2 position
+# guides, then per schedule the lighting kernels (1: reuse, spatial, march,
+# combine; 2: reuse, shade; 0: the 8 reference passes), then SVGF temporal,
+# variance and 4 a-trous.
+KERNELS_PER_FRAME = {1: 1 + 2 + 4 + 6, 2: 1 + 2 + 2 + 6, 0: 1 + 2 + 8 + 6}
 # Counted FP32 work of the march per oracle work counter (flops): BVH node
 # visit (box test), certified-box distance, field distance (transform,
 # trilinear, bounds), march step (penumbra update).
@@ -96,7 +127,7 @@ def workload_spec(args):
     return preset_spec(args.config, **over)
 
 
-def describe(spec, frames, schedule):
+def describe(spec, frames, schedule, storage):
     return {
         "workload": f"room of {6 if not spec.room_single_mesh else 1}+{spec.n_boxes}+{spec.n_spheres} meshes, "
                     f"{spec.width}x{spec.height}, {frames} frames",
@@ -105,9 +136,10 @@ def describe(spec, frames, schedule):
         "sdf": f"{spec.sdf_resolution}^3 {'f16' if spec.sdf_format else 'f32'}",
         "emitters": spec.n_lights, "vpl_paths": spec.vpl_count, "bounces": spec.vpl_bounces,
         "restir": "8+8 candidates, 4 neighbours r=12, 4-frame history", "sdf_march": "96 steps, eps 0.001, k=16",
-        "svgf": "32-frame history, 4 a-trous", "storage": "f32 G-buffer, f32 radiance, f32 moments",
+        "svgf": "32-frame history, 4 a-trous", "storage": storage,
         "schedule": schedule,
-        "l2": "inputs larger than L2: a distinct 120 MB G-buffer per frame, ~1 GB working set per frame",
+        "l2": "inputs larger than L2: a distinct G-buffer per frame (120 MB f32, 46 MB packed at 1920x1200) "
+              "and a 0.7-1.3 GB working set per frame",
         "parallelism": "replicas",
     }
 
@@ -216,11 +248,12 @@ def measured_peak():
         return 6650.0, "fallback"
 
 
-def ncu_traffic(kernel):
-    """DRAM bytes (read + write) per launch of `kernel` at 1920x1200 from the
-    committed ncu summary profiles/<kernel>_kernel_1920x1200.md (its line
-    `dram_bytes_per_launch: N`), or None when no capture is committed."""
-    path = os.path.join(ROOT, "profiles", f"{kernel}_kernel_1920x1200.md")
+def ncu_traffic(kernel, workload):
+    """DRAM bytes (read + write) per launch of `kernel` on `workload` (e.g.
+    "1920x1200") from the committed ncu summary
+    profiles/<kernel>_kernel_<workload>.md (its line `dram_bytes_per_launch: N`),
+    or None when no capture of that workload is committed."""
+    path = os.path.join(ROOT, "profiles", f"{kernel}_kernel_{workload}.md")
     try:
         for line in open(path):
             if line.startswith("dram_bytes_per_launch:"):
@@ -258,7 +291,7 @@ def cpu_run(spec, steps, warmup, budget_s, threads=0):
         y0 = (H - rows) // 2
         orc.set_rows(y0, y0 + rows)
         t = time.perf_counter()
-        orc.frame(f, OracleScene(obj, wl.meshes, nodes, lights, wl.atlas), g, v, p,
+        orc.frame(f, OracleScene(obj, wl.meshes, nodes, lights, wl.atlas_f32()), g, v, p,
                   wl.settings.svgf_iterations)
         dt = time.perf_counter() - t
         prev = v
@@ -297,7 +330,8 @@ def reference_arm(args):
         "steps": args.steps, "warmup": args.warmup, "ms_per_step": 1000.0 * r["seconds"] / r["steps"],
         "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f32", "data": "synthetic",
         "impl": "reference",
-        "config": describe(spec, frames, "CPU restatement of the WGSL passes (oracle/), OpenMP over pixels"),
+        "config": describe(spec, frames, "CPU restatement of the WGSL passes (oracle/), OpenMP over pixels",
+                           "f32 throughout (the oracle's arithmetic); f16 SDF texels dequantised"),
         "cpu_baseline": {"value": r["value"], "unit": "Mpix-frames/s", "cores": r["threads"], "kind": "port",
                          "sample": r["sample"]},
         "e2e": {"value": r["value"], "unit": "Mpix-frames/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
@@ -336,7 +370,9 @@ def ours(args):
     ctx = Context(dev)
     scene = Scene(ctx, wl.meshes, wl.atlas, wl.sdf_format)
     schedule = args.schedule
-    sess = Session(ctx, session_desc(wl.settings, L.GBUFFER_F32, L.RADIANCE_F32, schedule, False))
+    gfmt, rfmt, mfmt, storage = storage_of(args.config)
+    alg = alg_bytes(gfmt, rfmt, mfmt)
+    sess = Session(ctx, session_desc(wl.settings, gfmt, rfmt, schedule, False, moments_format=mfmt))
     stream = torch.cuda.current_stream()
     sh = stream_handle()
 
@@ -344,8 +380,8 @@ def ours(args):
     frames, gbufs, vpls = [], [], []
     for i in range(n_frames):
         f, obj, nodes, lights = wl.frame(i)
-        t, gs = gbuffer_device_alloc(H, W, L.GBUFFER_F32)
-        L.check(L.lib.irt_gbuffer_render(ctx.handle, wl.handle, C.byref(f), None, L.GBUFFER_F32, gs.depth,
+        t, gs = gbuffer_device_alloc(H, W, gfmt)
+        L.check(L.lib.irt_gbuffer_render(ctx.handle, wl.handle, C.byref(f), None, gfmt, gs.depth,
                                          gs.normal, gs.color, gs.params, gs.motion, sh), ctx.handle, "gbuffer")
         v = wl.vpls_cpu(f, obj, lights)
         frames.append((f, obj, nodes, lights))
@@ -406,10 +442,10 @@ def ours(args):
         for i in range(ring):
             f, obj, nodes, lights = frames[Wm + i] if Wm + i < n_frames else frames[i]
             g = {k: torch.from_numpy(v.view(np.uint8) if v.dtype != np.uint8 else v).pin_memory()
-                 for k, v in wl.gbuffer_cpu(f, L.GBUFFER_F32).items()}
+                 for k, v in wl.gbuffer_cpu(f, gfmt).items()}
             v = torch.from_numpy(wl.vpls_cpu(f, obj, lights).view(np.uint8)).pin_memory()
             host.append((f, obj, nodes, lights, g, v))
-        dev_g, dev_gs = gbuffer_device_alloc(H, W, L.GBUFFER_F32)
+        dev_g, dev_gs = gbuffer_device_alloc(H, W, gfmt)
         dv = [torch.empty_like(vpls[0]), torch.empty_like(vpls[0])]
         out_ptr, out_bytes = sess.buffer_ptr(L.BUF_FILTERED)
         out_dev = sess.buffer(L.BUF_FILTERED, torch.uint8)
@@ -465,14 +501,14 @@ def ours(args):
     peak, peak_kind = measured_peak()
 
     def ach(n):
-        return ALG_BYTES[n] * P / (mean_ms[kernel_idx[n]] / 1000.0) / 1e9
+        return alg[n] * P / (mean_ms[kernel_idx[n]] / 1000.0) / 1e9
 
     march_flops = None
     if counters:
         march_flops = sum(FLOPS_PER[k] * counters.get(k, 0.0) for k in FLOPS_PER)
     roofline = {"bound": "hbm", "kernel": dominant, "achieved": ach(dominant), "peak": peak, "unit": "GB/s",
-                "frac": ach(dominant) / peak, "traffic": ncu_traffic(dominant), "peak_source": peak_kind,
-                "alg_bytes_per_pixel": ALG_BYTES[dominant],
+                "frac": ach(dominant) / peak, "traffic": ncu_traffic(dominant, f"{W}x{H}" + ("_mixed" if args.config == 2 else "")), "peak_source": peak_kind,
+                "alg_bytes_per_pixel": alg[dominant],
                 "kernels": {n: {"ms": float(mean_ms[kernel_idx[n]]), "alg_GBps": ach(n), "frac": ach(n) / peak}
                             for n in KERNELS}}
     if march_flops is not None:
@@ -489,11 +525,11 @@ def ours(args):
             "metric": "Mpix-frames/s", "value": value, "unit": "Mpix-frames/s", "n_gpus": world, "steps": K,
             "warmup": Wm, "ms_per_step": ms_max / K, "higher_is_better": True, "scaling": "weak",
             "vs_baseline": None, "dtype": "f32", "data": "synthetic",
-            "config": describe(spec, n_frames, {1: "ray-queue", 2: "fused-inline", 0: "plain"}[schedule]),
+            "config": describe(spec, n_frames, {1: "ray-queue", 2: "fused-inline", 0: "plain"}[schedule], storage),
             "p50_frame_ms": float(np.percentile(frame_ms, 50)), "p99_frame_ms": float(np.percentile(frame_ms, 99)),
             "stage_ms": {n: float(mean_ms[i]) for i, n in enumerate(names)},
             "roofline": roofline, "cpu_baseline": cpu, "e2e": e2e,
-            "gpu_launches": K * {1: KERNELS_PER_FRAME, 2: 8, 0: 14}[schedule],
+            "gpu_launches": K * KERNELS_PER_FRAME[schedule],
             "clocks": clk,
         }
         print(json.dumps(line), flush=True)

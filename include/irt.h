@@ -156,8 +156,11 @@ irt_status irt_settings_validate(const irt_settings* s, char* msg, size_t msg_le
 
 /* SVGF moments / history length:
  *   F32: f32x4 (m1, m2, age, 0) — the reference's Rgba32Float;
- *   F16: f16x4 (m1, variance, age, 0) — compensated: the variance is kept
- *        instead of E[x^2] so HDR luminance^2 cannot overflow f16.          */
+ *   F16: 8 bytes — f16 mean and f16 standard deviation of the luminance,
+ *        then the history length as f32.  The second moment is stored
+ *        central (a deviation, not E[x^2]), so HDR luminance^2 cannot
+ *        overflow f16; the kernels combine moments in f32 with compensated
+ *        (shifted / pooled-variance) forms of E[x^2] - E[x]^2.              */
 #define IRT_MOMENTS_F32 0
 #define IRT_MOMENTS_F16 1
 

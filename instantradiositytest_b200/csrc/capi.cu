@@ -61,7 +61,7 @@ struct irt_session {
     irt_session_desc desc{};
     uint32_t W = 0, H = 0;
     size_t P = 0;
-    size_t rad_bytes = 0, normal_bytes = 0;
+    size_t rad_bytes = 0, normal_bytes = 0, mom_bytes = 0;
     irt_reservoir* dres[3] = {nullptr, nullptr, nullptr};
     irt_reservoir* ires[3] = {nullptr, nullptr, nullptr};
     irt_vpl* archive = nullptr;
@@ -441,7 +441,7 @@ uint64_t irt_session_bytes(const irt_session_desc* d) {
     b += P * 4 + P * normal_bytes_of(d->gbuffer_format);                            // previous depth/normal
     b += P * 16;                                                                    // direct f32x4
     b += P * rad * 7;  // noisy, feedback x2, temporal, scratch x2, filtered
-    b += P * 16 * 2;   // moments x2
+    b += P * (d->moments_format == IRT_MOMENTS_F16 ? 8 : 16) * 2;  // moments x2
     b += 16;           // error word
     if (d->fused == 1) b += P * (2 * sizeof(RayRecord) + 2 * 4 + 2 * 16) + 16;  // ray queue, vis, pending
     b += P * 16 * 2;                                                             // position guides
@@ -458,7 +458,7 @@ irt_status irt_session_create(irt_context* ctx, const irt_session_desc* desc, ir
     }
     if (desc->gbuffer_format < IRT_GBUFFER_F32 || desc->gbuffer_format > IRT_GBUFFER_PACKED ||
         (desc->radiance_format != IRT_RADIANCE_F32 && desc->radiance_format != IRT_RADIANCE_F16) ||
-        desc->moments_format != IRT_MOMENTS_F32) {
+        (desc->moments_format != IRT_MOMENTS_F32 && desc->moments_format != IRT_MOMENTS_F16)) {
         ctx->set_error("unsupported storage format");
         return IRT_E_INVALID;
     }
@@ -484,6 +484,7 @@ irt_status irt_session_create(irt_context* ctx, const irt_session_desc* desc, ir
     s->H = desc->settings.render_height;
     s->P = (size_t)s->W * s->H;
     s->rad_bytes = desc->radiance_format == IRT_RADIANCE_F16 ? 8 : 16;
+    s->mom_bytes = desc->moments_format == IRT_MOMENTS_F16 ? 8 : 16;
     s->normal_bytes = normal_bytes_of(desc->gbuffer_format);
     s->bytes = need;
     uint64_t used = 0;
@@ -505,7 +506,7 @@ irt_status irt_session_create(irt_context* ctx, const irt_session_desc* desc, ir
     if (!st) st = dev_alloc(ctx, &s->direct, P * 16, used);
     if (!st) st = dev_alloc(ctx, &s->noisy, P * s->rad_bytes, used);
     for (int k = 0; k < 2 && !st; k++) {
-        st = dev_alloc(ctx, &s->moments[k], P * 16, used);
+        st = dev_alloc(ctx, &s->moments[k], P * s->mom_bytes, used);
         if (!st) st = dev_alloc(ctx, &s->feedback[k], P * s->rad_bytes, used);
         if (!st) st = dev_alloc(ctx, &s->scratch[k], P * s->rad_bytes, used);
     }
@@ -722,6 +723,7 @@ irt_status irt_frame_svgf(irt_session* s, const irt_frame* f, const irt_gbuffer*
         L.guide = s->guide[0];
         L.old_guide = s->guide[1];
         L.radiance_f16 = s->desc.radiance_format == IRT_RADIANCE_F16;
+        L.moments_f16 = s->desc.moments_format == IRT_MOMENTS_F16;
         L.in = s->noisy;
         L.aux = s->feedback[old];
         L.moments_in = s->moments[old];
@@ -781,8 +783,8 @@ irt_status irt_session_buffer(irt_session* s, int32_t which, void** ptr, uint64_
     case IRT_BUF_DIRECT: p = s->direct; b = P * 16; break;
     case IRT_BUF_NOISY: p = s->noisy; b = P * s->rad_bytes; break;
     case IRT_BUF_FILTERED: p = s->filtered; b = P * s->rad_bytes; break;
-    case IRT_BUF_MOMENTS: p = s->moments[cur]; b = P * 16; break;
-    case IRT_BUF_MOMENTS_OLD: p = s->moments[old]; b = P * 16; break;
+    case IRT_BUF_MOMENTS: p = s->moments[cur]; b = P * s->mom_bytes; break;
+    case IRT_BUF_MOMENTS_OLD: p = s->moments[old]; b = P * s->mom_bytes; break;
     case IRT_BUF_FEEDBACK: p = s->feedback[cur]; b = P * s->rad_bytes; break;
     case IRT_BUF_FEEDBACK_OLD: p = s->feedback[old]; b = P * s->rad_bytes; break;
     case IRT_BUF_VPL_ARCHIVE:

@@ -33,6 +33,42 @@ struct Guide {
     float m0, m1, pixel_scale;
 };
 
+// Moment history storage.
+//  MomF32: the reference's Rgba32Float (E[l], E[l^2], history length, 0).
+//  MomF16: 8 bytes — mean and standard deviation of the luminance as two
+//    halves, the history length as f32.  The second moment is kept central
+//    (a deviation, not E[l^2]), so the f16 range holds it (luminance is
+//    clamped at 65000; E[l^2] would overflow at 256) and the variance is
+//    never formed as a difference of two rounded f16 values.  The kernels
+//    accumulate and combine in f32 with the compensated forms below.
+struct Moments {
+    float mean, second, age;  // MomF32: second = E[l^2]; MomF16: second = deviation
+};
+struct MomF32 {
+    typedef float4 T;
+    static constexpr bool central = false;
+    __device__ __forceinline__ static Moments load(const T* p, size_t i) {
+        float4 m = p[i];
+        return Moments{m.x, m.y, m.z};
+    }
+    __device__ __forceinline__ static void store(T* p, size_t i, Moments m) {
+        p[i] = make_float4(m.mean, m.second, m.age, 0.f);
+    }
+};
+struct MomF16 {
+    typedef uint2 T;
+    static constexpr bool central = true;
+    __device__ __forceinline__ static Moments load(const T* p, size_t i) {
+        uint2 m = p[i];
+        __half2 h = *reinterpret_cast<const __half2*>(&m.x);
+        return Moments{__low2float(h), __high2float(h), __uint_as_float(m.y)};
+    }
+    __device__ __forceinline__ static void store(T* p, size_t i, Moments m) {
+        __half2 h = __floats2half2_rn(m.mean, m.second);
+        p[i] = make_uint2(*reinterpret_cast<const uint32_t*>(&h), __float_as_uint(m.age));
+    }
+};
+
 template <class G>
 struct Sv {
     const irt_frame& f;
@@ -92,6 +128,22 @@ struct Sv {
         return wn * wz * wc;
     }
 };
+
+// Calls fn(G{}, R{}, M{}) with the G-buffer, radiance and moment storage
+// types a launch names.
+template <class Fn>
+__host__ inline cudaError_t dispatch_svgf(const SvgfLaunch& L, Fn&& fn) {
+    auto with_m = [&](auto g, auto r) {
+        return L.moments_f16 ? fn(g, r, MomF16{}) : fn(g, r, MomF32{});
+    };
+    auto with_r = [&](auto g) { return L.radiance_f16 ? with_m(g, RadF16{}) : with_m(g, RadF32{}); };
+    switch (L.gbuffer.format) {
+    case IRT_GBUFFER_F32: return with_r(GbF32{});
+    case IRT_GBUFFER_F16: return with_r(GbF16{});
+    case IRT_GBUFFER_PACKED: return with_r(GbPacked{});
+    }
+    return cudaErrorInvalidValue;
+}
 
 template <class G>
 __host__ inline SvgfCtx<G> make_ctx(const SvgfLaunch& L) {

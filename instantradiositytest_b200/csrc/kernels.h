@@ -106,6 +106,7 @@ struct SvgfLaunch {
     void* moments_out;       // temporal: current moments
     int step;
     int radiance_f16;
+    int moments_f16;          // moments: 0 float4 (E[l], E[l^2], age, 0); 1 MomF16 (half mean, half deviation, f32 age)
     const float4* guide;      // per-pixel positions of this frame (or null)
     const float4* old_guide;  // ... of the previous frame (or null)
 };

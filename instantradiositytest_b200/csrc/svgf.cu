@@ -12,11 +12,16 @@
 namespace irtd {
 
 // svgf.wgsl:45-76
-template <class G, class R>
+// With MomF16 the moment history is (mean, deviation) and the blend of
+// history and the current sample is done on central moments (the pooled
+// variance of the bilinear taps about their mean, then
+// (1-b)*var_h + b*(1-b)*(l - mean_h)^2), which equals the reference's
+// E[l^2] - E[l]^2 without its cancellation.
+template <class G, class R, class M>
 __global__ void __launch_bounds__(256) svgf_temporal_kernel(const __grid_constant__ irt_frame f, const __grid_constant__ SvgfCtx<G> c,
                                                             const typename R::T* noisy, const typename R::T* old_radiance,
-                                                            const float4* old_moments, typename R::T* radiance_out,
-                                                            float4* moments_out) {
+                                                            const typename M::T* old_moments, typename R::T* radiance_out,
+                                                            typename M::T* moments_out) {
     int32_t x = blockIdx.x * blockDim.x + threadIdx.x;
     int32_t y = blockIdx.y * blockDim.y + threadIdx.y;
     Sv<G> sv(f, c);
@@ -27,6 +32,7 @@ __global__ void __launch_bounds__(256) svgf_temporal_kernel(const __grid_constan
     float l = luminance(cc);
     V3 history = V3{0.f, 0.f, 0.f};
     float hm0 = 0.f, hm1 = 0.f, length_history = 0.f, total = 0.f;
+    float tap_w[4] = {0.f, 0.f, 0.f, 0.f}, tap_mean[4], tap_dev[4];  // MomF16 only
     if (c.g.d(i) < 1.f) {
         float2 mv = c.g.mv(i);
         float px = (sv.uvx(x) - mv.x) * (float)sv.W - .5f;
@@ -41,16 +47,22 @@ __global__ void __launch_bounds__(256) svgf_temporal_kernel(const __grid_constan
                 int32_t qx = bx + xx, qy = by + yy;
                 if (!sv.history_ok(x, y, qx, qy)) continue;
                 size_t q = sv.idx(qx, qy);
-                float4 m = old_moments[q];
-                if (m.z <= 0.f) continue;
+                Moments m = M::load(old_moments, q);
+                if (m.age <= 0.f) continue;
                 float wx = xx == 1 ? fx : 1.f - fx;
                 float wy = yy == 1 ? fy : 1.f - fy;
                 float w = wx * wy;
                 float4 h = R::load(old_radiance, q);
                 history = history + V3{h.x, h.y, h.z} * w;
-                hm0 += m.x * w;
-                hm1 += m.y * w;
-                length_history += m.z * w;
+                hm0 += m.mean * w;
+                if constexpr (M::central) {
+                    tap_w[yy * 2 + xx] = w;
+                    tap_mean[yy * 2 + xx] = m.mean;
+                    tap_dev[yy * 2 + xx] = m.second;
+                } else {
+                    hm1 += m.second * w;
+                }
+                length_history += m.age * w;
                 total += w;
             }
     }
@@ -81,14 +93,30 @@ __global__ void __launch_bounds__(256) svgf_temporal_kernel(const __grid_constan
         result = V3{history.x * (1.f - alpha) + cc.x * alpha, history.y * (1.f - alpha) + cc.y * alpha,
                     history.z * (1.f - alpha) + cc.z * alpha};
         float beta = wmax(.2f, 1.f / age);
-        float n0 = hm0 * (1.f - beta) + m0 * beta;
-        float n1 = hm1 * (1.f - beta) + m1 * beta;
-        m0 = n0;
-        m1 = n1;
+        if constexpr (M::central) {
+            float var_h = 0.f;
+#pragma unroll
+            for (int k = 0; k < 4; k++) {
+                if (tap_w[k] == 0.f) continue;
+                float d = tap_mean[k] - hm0;
+                var_h += (tap_dev[k] * tap_dev[k] + d * d) * tap_w[k];
+            }
+            var_h /= total;
+            float d = l - hm0;
+            m0 = hm0 * (1.f - beta) + l * beta;
+            m1 = var_h * (1.f - beta) + d * d * (beta * (1.f - beta));  // central: the variance
+        } else {
+            float n0 = hm0 * (1.f - beta) + m0 * beta;
+            float n1 = hm1 * (1.f - beta) + m1 * beta;
+            m0 = n0;
+            m1 = n1;
+        }
+    } else if constexpr (M::central) {
+        m1 = 0.f;
     }
-    float variance = wmax(m1 - m0 * m0, 0.f);
+    float variance = M::central ? m1 : wmax(m1 - m0 * m0, 0.f);
     R::store(radiance_out, i, make_float4(result.x, result.y, result.z, wmin(sqrtf(variance), 65000.f)));
-    moments_out[i] = make_float4(m0, m1, age, 0.f);
+    M::store(moments_out, i, Moments{m0, M::central ? sqrtf(variance) : m1, age});
 }
 
 // World position of every pixel, world(pixel_uv, depth, inv_vp)
@@ -111,7 +139,7 @@ __global__ void __launch_bounds__(256) guide_kernel(const __grid_constant__ irt_
     out[i] = make_float4(p.x, p.y, p.z, s);
 }
 
-template <class G, class R>
+template <class G, class R, class M>
 static cudaError_t svgf_typed(const SvgfLaunch& L, int stage, cudaStream_t st) {
     SvgfCtx<G> c = make_ctx<G>(L);
     const irt_frame& f = *L.frame;
@@ -120,8 +148,9 @@ static cudaError_t svgf_typed(const SvgfLaunch& L, int stage, cudaStream_t st) {
     dim3 grid((f.size[0] + 31) / 32, (f.size[1] + 7) / 8);
     switch (stage) {
     case 0:
-        svgf_temporal_kernel<G, R><<<grid, block, 0, st>>>(f, c, (const T*)L.in, (const T*)L.aux, (const float4*)L.moments_in,
-                                                           (T*)L.out, (float4*)L.moments_out);
+        svgf_temporal_kernel<G, R, M><<<grid, block, 0, st>>>(f, c, (const T*)L.in, (const T*)L.aux,
+                                                              (const typename M::T*)L.moments_in, (T*)L.out,
+                                                              (typename M::T*)L.moments_out);
         break;
     case 3:
     case 4: {
@@ -139,18 +168,9 @@ static cudaError_t svgf_typed(const SvgfLaunch& L, int stage, cudaStream_t st) {
 cudaError_t irt_launch_svgf(const SvgfLaunch& L, int stage, cudaStream_t st) {
     using namespace irtd;
     if (stage == 1 || stage == 2) return irt_launch_svgf_spatial(L, stage, st);
-    if (L.radiance_f16) {
-        switch (L.gbuffer.format) {
-        case IRT_GBUFFER_F32: return svgf_typed<GbF32, RadF16>(L, stage, st);
-        case IRT_GBUFFER_F16: return svgf_typed<GbF16, RadF16>(L, stage, st);
-        case IRT_GBUFFER_PACKED: return svgf_typed<GbPacked, RadF16>(L, stage, st);
-        }
-    } else {
-        switch (L.gbuffer.format) {
-        case IRT_GBUFFER_F32: return svgf_typed<GbF32, RadF32>(L, stage, st);
-        case IRT_GBUFFER_F16: return svgf_typed<GbF16, RadF32>(L, stage, st);
-        case IRT_GBUFFER_PACKED: return svgf_typed<GbPacked, RadF32>(L, stage, st);
-        }
-    }
-    return cudaErrorInvalidValue;
+    if (stage == 3 || stage == 4)  // guides read neither radiance nor moments
+        return svgf_typed<GbF32, RadF32, MomF32>(L, stage, st);
+    return dispatch_svgf(L, [&](auto g, auto r, auto m) {
+        return svgf_typed<decltype(g), decltype(r), decltype(m)>(L, stage, st);
+    });
 }

@@ -12,9 +12,12 @@
 namespace irtd {
 
 // svgf.wgsl:77-89
-template <class G, class R>
+// With MomF16 (mean, deviation) moments the 7x7 sums are taken about the
+// centre pixel's mean (shifted data), so E[l^2] - E[l]^2 is formed from
+// small numbers: s0 = sum w (m - K), s1 = sum w (dev^2 + (m - K)^2).
+template <class G, class R, class M>
 __global__ void __launch_bounds__(256) svgf_variance_kernel(const __grid_constant__ irt_frame f, const __grid_constant__ SvgfCtx<G> c,
-                                                            const typename R::T* input, const float4* moments,
+                                                            const typename R::T* input, const typename M::T* moments,
                                                             typename R::T* out) {
     int32_t x = blockIdx.x * blockDim.x + threadIdx.x;
     int32_t y = blockIdx.y * blockDim.y + threadIdx.y;
@@ -22,19 +25,27 @@ __global__ void __launch_bounds__(256) svgf_variance_kernel(const __grid_constan
     if (x >= sv.W || y >= sv.H) return;
     size_t i = sv.idx(x, y);
     float4 in = R::load(input, i);
-    float age = moments[i].z;
+    Moments centre = M::load(moments, i);
+    float age = centre.age;
     float sigma = in.w;
     if (age < 4.f && c.g.d(i) < 1.f) {
         float s0 = 0.f, s1 = 0.f, total = 0.f;
+        const float K = M::central ? centre.mean : 0.f;
         Guide a = sv.guide(x, y);
         for (int32_t yy = -3; yy <= 3; yy++)
             for (int32_t xx = -3; xx <= 3; xx++) {
                 int32_t qx = x + xx, qy = y + yy;
                 float w = sv.geometry_weight(a, qx, qy, 1.f);
                 if (w <= 0.f) continue;
-                float4 m = moments[sv.idx(qx, qy)];
-                s0 += m.x * w;
-                s1 += m.y * w;
+                Moments m = M::load(moments, sv.idx(qx, qy));
+                if constexpr (M::central) {
+                    float d = m.mean - K;
+                    s0 += d * w;
+                    s1 += (m.second * m.second + d * d) * w;
+                } else {
+                    s0 += m.mean * w;
+                    s1 += m.second * w;
+                }
                 total += w;
             }
         float dn = wmax(total, .00001f);
@@ -102,7 +113,7 @@ __global__ void __launch_bounds__(256) svgf_atrous_kernel(const __grid_constant_
     if (out2) R::store(out2, i, o);
 }
 
-template <class G, class R>
+template <class G, class R, class M>
 static cudaError_t spatial_typed(const SvgfLaunch& L, int stage, cudaStream_t st) {
     SvgfCtx<G> c = make_ctx<G>(L);
     const irt_frame& f = *L.frame;
@@ -110,7 +121,8 @@ static cudaError_t spatial_typed(const SvgfLaunch& L, int stage, cudaStream_t st
     dim3 block(32, 8);
     dim3 grid((f.size[0] + 31) / 32, (f.size[1] + 7) / 8);
     if (stage == 1)
-        svgf_variance_kernel<G, R><<<grid, block, 0, st>>>(f, c, (const T*)L.in, (const float4*)L.moments_in, (T*)L.out);
+        svgf_variance_kernel<G, R, M><<<grid, block, 0, st>>>(f, c, (const T*)L.in,
+                                                              (const typename M::T*)L.moments_in, (T*)L.out);
     else if (stage == 2)
         svgf_atrous_kernel<G, R><<<grid, block, 0, st>>>(f, c, (const T*)L.in, (T*)L.out, (T*)L.out2, L.step);
     else
@@ -122,18 +134,14 @@ static cudaError_t spatial_typed(const SvgfLaunch& L, int stage, cudaStream_t st
 
 cudaError_t irt_launch_svgf_spatial(const SvgfLaunch& L, int stage, cudaStream_t st) {
     using namespace irtd;
-    if (L.radiance_f16) {
-        switch (L.gbuffer.format) {
-        case IRT_GBUFFER_F32: return spatial_typed<GbF32, RadF16>(L, stage, st);
-        case IRT_GBUFFER_F16: return spatial_typed<GbF16, RadF16>(L, stage, st);
-        case IRT_GBUFFER_PACKED: return spatial_typed<GbPacked, RadF16>(L, stage, st);
-        }
-    } else {
-        switch (L.gbuffer.format) {
-        case IRT_GBUFFER_F32: return spatial_typed<GbF32, RadF32>(L, stage, st);
-        case IRT_GBUFFER_F16: return spatial_typed<GbF16, RadF32>(L, stage, st);
-        case IRT_GBUFFER_PACKED: return spatial_typed<GbPacked, RadF32>(L, stage, st);
-        }
+    if (stage == 2) {  // a-trous reads no moments
+        SvgfLaunch A = L;
+        A.moments_f16 = 0;
+        return dispatch_svgf(A, [&](auto g, auto r, auto) {
+            return spatial_typed<decltype(g), decltype(r), MomF32>(A, stage, st);
+        });
     }
-    return cudaErrorInvalidValue;
+    return dispatch_svgf(L, [&](auto g, auto r, auto m) {
+        return spatial_typed<decltype(g), decltype(r), decltype(m)>(L, stage, st);
+    });
 }

@@ -356,7 +356,13 @@ bool Workload::build() {
         irt_light li{};
         li.position_strength[0] = (float)x;
         li.position_strength[1] = (float)y;
-        li.position_strength[2] = (float)(kRoomHalf - kWallHalf - 0.05);
+        // 0.05 m below the ceiling when the walls are certified boxes (exact
+        // distances).  A room that is one field mesh has the field bias
+        // voxel diagonal * (0.5 + 1/128) (~0.07 m at 128^3 over the room)
+        // plus the march clearance (0.65 voxel) around its surface, so a
+        // light closer than ~0.13 m would sit inside it and every shadow ray
+        // to it would end occluded: those emitters hang 0.5 m below.
+        li.position_strength[2] = (float)(kRoomHalf - kWallHalf - (spec.room_single_mesh ? 0.5 : 0.05));
         li.position_strength[3] = (float)(L * size * size);
         li.direction_angle[0] = 0.f;
         li.direction_angle[1] = 0.f;

@@ -81,8 +81,8 @@ class Scene:
 
 
 def session_desc(settings: L.Settings, gbuffer_format=L.GBUFFER_F32, radiance_format=L.RADIANCE_F32, fused=True,
-                 keep_candidates=False, exact_march=False) -> L.SessionDesc:
-    return L.SessionDesc(settings, gbuffer_format, radiance_format, L.MOMENTS_F32, int(fused), int(keep_candidates),
+                 keep_candidates=False, exact_march=False, moments_format=L.MOMENTS_F32) -> L.SessionDesc:
+    return L.SessionDesc(settings, gbuffer_format, radiance_format, moments_format, int(fused), int(keep_candidates),
                          int(exact_march))
 
 
@@ -138,6 +138,22 @@ class Session:
             return raw.view(np.float16).astype(np.float32).reshape(self.h, self.w, 4)
         return raw.view(np.float32).reshape(self.h, self.w, 4)
 
+    def moments_host(self, which=L.BUF_MOMENTS) -> np.ndarray:
+        """Moments as the reference's (E[l], E[l^2], age, 0) float32 [H, W, 4],
+        whatever the storage format."""
+        p, n = self.buffer_ptr(which)
+        raw = device_tensor(p, n, torch.uint8).cpu().numpy()
+        if n == self.w * self.h * 16:
+            return raw.view(np.float32).reshape(self.h, self.w, 4)
+        rec = raw.view(np.dtype([("mean", "<f2"), ("dev", "<f2"), ("age", "<f4")])).reshape(self.h, self.w)
+        out = np.zeros((self.h, self.w, 4), np.float32)
+        mean = rec["mean"].astype(np.float32)
+        dev = rec["dev"].astype(np.float32)
+        out[..., 0] = mean
+        out[..., 1] = dev * dev + mean * mean
+        out[..., 2] = rec["age"]
+        return out
+
     def check(self, stream=None):
         return lib.irt_session_check(self.handle, stream if stream is not None else stream_handle())
 
@@ -186,14 +202,14 @@ class FrameDriver:
 
     def __init__(self, wl: Workload, ctx: Context | None = None, gbuffer_format=L.GBUFFER_F32,
                  radiance_format=L.RADIANCE_F32, fused=True, keep_candidates=False, gpu_gbuffer=False,
-                 exact_march=False):
+                 exact_march=False, moments_format=L.MOMENTS_F32):
         self.wl = wl
         self.ctx = ctx or Context()
         self.own_ctx = ctx is None
         self.fmt = gbuffer_format
         self.scene = Scene(self.ctx, wl.meshes, wl.atlas, wl.sdf_format)
         self.session = Session(self.ctx, session_desc(wl.settings, gbuffer_format, radiance_format, fused,
-                                                      keep_candidates, exact_march))
+                                                      keep_candidates, exact_march, moments_format))
         self.gpu_gbuffer = gpu_gbuffer
         self.prev_vpls = None
         self.last = None

@@ -55,6 +55,19 @@ class Workload:
             raw = np.frombuffer((C.c_float * n).from_address(ap), dtype=np.float32)
         self.atlas = raw.reshape(dims[2], dims[1], dims[0]).copy()
 
+    def atlas_f32(self) -> np.ndarray:
+        """The SDF texels the kernels see, as f32: F16 atlases dequantised
+        with each mesh tile's scale (irt_mesh.lo[3])."""
+        if self.sdf_format == L.SDF_F32:
+            return self.atlas
+        if getattr(self, "_atlas_f32", None) is None:
+            out = self.atlas.view(np.float16).astype(np.float32)
+            for m in self.meshes:
+                x, y, z, r = (int(v) for v in m["field"])
+                out[z:z + r, y:y + r, x:x + r] *= np.float32(m["lo"][3])
+            self._atlas_f32 = out
+        return self._atlas_f32
+
     def close(self):
         if self.handle:
             lib.irt_workload_destroy(self.handle)

@@ -58,31 +58,54 @@ def sync_history(orc: Oracle, drv: FrameDriver, prev_index: int):
         pn = np.concatenate([n3, np.zeros(n3.shape[:-1] + (1,), np.float32)], -1).reshape(-1)
     orc.buffer(ob.PREV_NORMAL)[:] = pn.reshape(-1)
     k = prev_index % 2
-    orc.buffer(ob.MOMENTS[k])[:] = s.image_host(L.BUF_MOMENTS).reshape(-1)
+    orc.buffer(ob.MOMENTS[k])[:] = s.moments_host(L.BUF_MOMENTS).reshape(-1)
     orc.buffer(ob.FEEDBACK[k])[:] = s.image_host(L.BUF_FEEDBACK).reshape(-1)
+
+
+def outputs(o: Oracle, index: int):
+    d = o.image(ob.DIRECT)[..., :3]
+    n = o.image(ob.LIGHTING)[..., :3]
+    return {"direct": d, "noisy": n, "indirect": n - d, "filtered": o.image(ob.HISTORIES[index % 2])[..., :3],
+            "moments": o.image(ob.MOMENTS[index % 2])[..., :3]}
 
 
 class Lockstep:
     def __init__(self, wl: Workload, gbuffer_format=L.GBUFFER_F32, radiance_format=L.RADIANCE_F32, fused=1,
-                 precision=0):
+                 precision=0, moments_format=L.MOMENTS_F32, oracle_f16_storage=None, f64_witness=False):
+        """precision 0: the oracle in f32 (the reference's arithmetic), 1: in
+        f64.  oracle_f16_storage: round the oracle's radiance history to f16
+        as the reference's Rgba16Float does (default: when the radiance
+        format is F16).  f64_witness: also run an f64 oracle without f16
+        storage from the same synced history, and report the error of the
+        CUDA outputs (`f64_<output>`) and of the primary oracle
+        (`floor_<output>`, the f32 arithmetic's own distance from f64)
+        against it."""
         self.wl = wl
         self.drv = FrameDriver(wl, gbuffer_format=gbuffer_format, radiance_format=radiance_format, fused=fused,
-                               keep_candidates=True)
-        self.orc = Oracle(wl.width, wl.height, wl.settings.vpl_count, wl.settings.restir_max_history, precision,
-                          radiance_format == L.RADIANCE_F16)
+                               keep_candidates=True, moments_format=moments_format)
+        if oracle_f16_storage is None:
+            oracle_f16_storage = radiance_format == L.RADIANCE_F16
+        args = (wl.width, wl.height, wl.settings.vpl_count, wl.settings.restir_max_history)
+        self.orc = Oracle(*args, precision, oracle_f16_storage)
+        self.witness = Oracle(*args, 1, False) if f64_witness else None
         self.fmt = gbuffer_format
         self.prev_vpls = None
+        self.atlas = atlas_f32(wl)
 
     def frame(self, index: int, sync=True, debug=0):
         inputs = self.drv.inputs(index, debug)
         f, obj, nodes, lights, planes, vpls = inputs
+        orcs = [o for o in (self.orc, self.witness) if o is not None]
         if sync and index > 0:
-            sync_history(self.orc, self.drv, index - 1)
+            for o in orcs:
+                sync_history(o, self.drv, index - 1)
         self.drv.step(index, debug, inputs=inputs)
         torch.cuda.synchronize()
         prev = self.prev_vpls if self.prev_vpls is not None else np.zeros_like(vpls)
-        sc = OracleScene(obj, self.wl.meshes, nodes, lights, atlas_f32(self.wl))
-        self.orc.frame(f, sc, gbuffer_as_f32(planes, self.fmt), vpls, prev, self.wl.settings.svgf_iterations)
+        sc = OracleScene(obj, self.wl.meshes, nodes, lights, self.atlas)
+        g = gbuffer_as_f32(planes, self.fmt)
+        for o in orcs:
+            o.frame(f, sc, g, vpls, prev, self.wl.settings.svgf_iterations)
         self.prev_vpls = vpls
         return self.compare(index)
 
@@ -93,26 +116,27 @@ class Lockstep:
             for k in (0, 1, 2):
                 out[f"select_{key}{k}"] = selection_match(s.reservoirs_host(dom, k),
                                                           o.reservoirs(key, k, L.RESERVOIR_DTYPE))
-        out["direct"] = rel_l1(s.image_host(L.BUF_DIRECT)[..., :3], o.image(ob.DIRECT)[..., :3])
-        out["noisy"] = rel_l1(s.image_host(L.BUF_NOISY)[..., :3], o.image(ob.LIGHTING)[..., :3])
-        out["filtered"] = rel_l1(s.image_host(L.BUF_FILTERED)[..., :3], o.image(ob.HISTORIES[index % 2])[..., :3])
-        out["moments"] = rel_l1(s.image_host(L.BUF_MOMENTS)[..., :3], o.image(ob.MOMENTS[index % 2])[..., :3])
+        direct = s.image_host(L.BUF_DIRECT)[..., :3]
+        noisy = s.image_host(L.BUF_NOISY)[..., :3]
+        ours = {"direct": direct, "noisy": noisy, "indirect": noisy - direct,
+                "filtered": s.image_host(L.BUF_FILTERED)[..., :3], "moments": s.moments_host(L.BUF_MOMENTS)[..., :3]}
+        ref = outputs(o, index)
+        for k in ours:
+            out[k] = rel_l1(ours[k], ref[k])
+        if self.witness is not None:
+            w = outputs(self.witness, index)
+            for k in ours:
+                out[f"f64_{k}"] = rel_l1(ours[k], w[k])
+                out[f"floor_{k}"] = rel_l1(ref[k], w[k])
         return out
 
     def close(self):
         self.drv.close()
         self.orc.close()
+        if self.witness is not None:
+            self.witness.close()
 
 
 def atlas_f32(wl: Workload) -> np.ndarray:
     """The SDF texels the kernels see, dequantised (f16 x per-mesh scale)."""
-    if wl.sdf_format == L.SDF_F32:
-        return wl.atlas
-    a = wl.atlas.view(np.float16).astype(np.float32)
-    out = np.empty_like(a)
-    # each mesh tile carries its own scale in irt_mesh.lo[3]
-    out[:] = a
-    for m in wl.meshes:
-        x, y, z, r = (int(v) for v in m["field"])
-        out[z:z + r, y:y + r, x:x + r] = a[z:z + r, y:y + r, x:x + r] * np.float32(m["lo"][3])
-    return out
+    return wl.atlas_f32()
