@@ -383,6 +383,14 @@ irt_status irt_gbuffer_render(irt_context* ctx, const irt_workload* wl, const ir
                               const irt_object* objects, int32_t format, float* depth,
                               void* normal, void* color, void* params, void* motion,
                               void* stream);
+/* CUDA VPL generator (replaces the vpl.wgsl compute pass, vpl.wgsl:1-47, and
+ * its dispatch in src/renderer.rs:1873-1884): frame->counts[1] paths of up to
+ * frame->counts[2] bounces from the lights last uploaded to `scene`
+ * (irt_scene_update), written to the device pool `out`.  Ray casts run
+ * against the workload's analytic primitives (the reference uses a hardware
+ * ray query against its TLAS).  Same contract as irt_workload_vpls_cpu. */
+irt_status irt_vpl_generate(irt_scene* scene, const irt_workload* wl, const irt_frame* frame,
+                            irt_vpl* out, void* stream);
 
 #ifdef __cplusplus
 }

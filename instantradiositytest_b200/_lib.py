@@ -164,6 +164,7 @@ _PROTOS = {
     "irt_workload_gbuffer_cpu": (I32, [P, C.POINTER(Frame), P, I32, P, P, P, P, P]),
     "irt_workload_vpls_cpu": (I32, [P, C.POINTER(Frame), P, P, P]),
     "irt_gbuffer_render": (I32, [P, P, C.POINTER(Frame), P, I32, P, P, P, P, P, P]),
+    "irt_vpl_generate": (I32, [P, P, C.POINTER(Frame), P, P]),
 }
 
 

@@ -412,6 +412,27 @@ irt_status irt_scene_update(irt_scene* sc, const irt_object* objects, uint32_t o
     return IRT_OK;
 }
 
+irt_status irt_vpl_generate(irt_scene* sc, const irt_workload* wl, const irt_frame* f, irt_vpl* out, void* stream) {
+    if (!sc || !wl || !f || !out) return IRT_E_INVALID;
+    irt_context* ctx = sc->ctx;
+    if (f->counts[0] > sc->light_count || (f->counts[0] && !sc->lights)) {
+        ctx->set_error("frame light count exceeds the scene's uploaded lights");
+        return IRT_E_INVALID;
+    }
+    if (f->counts[2] > 64) {
+        ctx->set_error("VPL bounce count out of range");
+        return IRT_E_INVALID;
+    }
+    DeviceGuard dg(ctx->device);
+    VplLaunch V{};
+    V.frame = f;
+    V.lights = sc->lights;
+    V.out = out;
+    CK(irt_workload_prims(wl, &V.prims, &V.n_prims), "workload primitives");
+    CK(irt_launch_vpls(V, static_cast<cudaStream_t>(stream)), "vpl kernel");
+    return IRT_OK;
+}
+
 void irt_scene_destroy(irt_scene* sc) {
     if (!sc) return;
     DeviceGuard g(sc->ctx->device);

@@ -78,6 +78,16 @@ struct Surface {
     float nv, a2, g1v, km;
     V3 f0;            // mix(vec3(.04), color, metal)
 };
+// The same for an explicit outgoing direction (a VPL path vertex: -ray).
+__device__ __forceinline__ void surface_terms_wo(Surface& s, V3 wo) {
+    s.wo = wo;
+    s.nv = wmax(dot(s.n, s.wo), .00001f);
+    float a = s.rough * s.rough;
+    s.a2 = a * a;
+    s.g1v = 2.f * s.nv / (s.nv + sqrtf(s.a2 + (1.f - s.a2) * s.nv * s.nv));
+    s.km = 1.f - s.metal;
+    s.f0 = V3{.04f * s.km + s.color.x * s.metal, .04f * s.km + s.color.y * s.metal, .04f * s.km + s.color.z * s.metal};
+}
 __device__ __forceinline__ void surface_terms(Surface& s, V3 camera) {
     s.wo = normalize(camera - s.p);
     s.nv = wmax(dot(s.n, s.wo), .00001f);

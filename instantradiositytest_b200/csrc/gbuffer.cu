@@ -6,6 +6,8 @@
 
 #include <vector>
 
+#include "dev_prims.cuh"
+#include "kernels.h"
 #include "workload.h"
 
 namespace {
@@ -47,67 +49,10 @@ __global__ void gbuffer_kernel(const __grid_constant__ irt_frame f, const GPrim*
     xf(f.inv_vp.m, nx, ny, 1.f, 1.f, pf);
     float o[3] = {pn[0] / pn[3], pn[1] / pn[3], pn[2] / pn[3]};
     float d[3] = {pf[0] / pf[3] - o[0], pf[1] / pf[3] - o[1], pf[2] / pf[3] - o[2]};
-    float best = 1.f;
-    int hit = -1;
+    // d spans near to far plane: t in [0, 1).
+    float best;
     float nl_best[3] = {0, 0, 0};
-    for (uint32_t k = 0; k < n_prims; k++) {
-        const GPrim& p = prims[k];
-        float lo4[4], ld4[4];
-        xf(p.inv_model, o[0], o[1], o[2], 1.f, lo4);
-        xf(p.inv_model, d[0], d[1], d[2], 0.f, ld4);
-        float t;
-        float nn[3] = {0, 0, 0};
-        bool h = false;
-        if (p.sphere) {
-            float r = p.lo[0];
-            float b = lo4[0] * ld4[0] + lo4[1] * ld4[1] + lo4[2] * ld4[2];
-            float a = ld4[0] * ld4[0] + ld4[1] * ld4[1] + ld4[2] * ld4[2];
-            float c = lo4[0] * lo4[0] + lo4[1] * lo4[1] + lo4[2] * lo4[2] - r * r;
-            float disc = b * b - a * c;
-            if (disc >= 0.f) {
-                t = (-b - sqrtf(disc)) / a;
-                if (t >= 0.f && t < best) {
-                    h = true;
-                    for (int q = 0; q < 3; q++) nn[q] = (lo4[q] + ld4[q] * t) / r;
-                }
-            }
-        } else {
-            float t0 = 0.f, t1 = best;
-            int axis = -1;
-            float sign = 0.f;
-            bool miss = false;
-            for (int a = 0; a < 3 && !miss; a++) {
-                float inv = 1.f / ld4[a];
-                float ta = (p.lo[a] - lo4[a]) * inv, tb = (p.hi[a] - lo4[a]) * inv;
-                float s = -1.f;
-                if (ta > tb) {
-                    float tmp = ta;
-                    ta = tb;
-                    tb = tmp;
-                    s = 1.f;
-                }
-                if (ta > t0) {
-                    t0 = ta;
-                    axis = a;
-                    sign = s;
-                }
-                t1 = fminf(t1, tb);
-                if (t0 > t1) miss = true;
-            }
-            if (!miss && axis >= 0 && t0 < best) {
-                h = true;
-                t = t0;
-                nn[axis] = sign;
-            }
-        }
-        if (h) {
-            best = t;
-            hit = (int)k;
-            nl_best[0] = nn[0];
-            nl_best[1] = nn[1];
-            nl_best[2] = nn[2];
-        }
-    }
+    int hit = irtd::cast_prims(prims, n_prims, o, d, 0.f, 1.f, best, nl_best);
     float dep = 1.f, nrm[3] = {0, 0, 0}, col[3] = {0, 0, 0}, par[2] = {0, 0}, mot[2] = {0, 0};
     if (hit >= 0) {
         const GPrim& p = prims[hit];
@@ -153,52 +98,65 @@ __global__ void gbuffer_kernel(const __grid_constant__ irt_frame f, const GPrim*
 
 }  // namespace
 
-extern "C" irt_status irt_gbuffer_render(irt_context* ctx, const irt_workload* wl_c, const irt_frame* f,
-                                         const irt_object* objects, int32_t format, float* depth, void* normal,
-                                         void* color, void* params, void* motion, void* stream) {
-    (void)objects;
-    if (!ctx || !wl_c || !f || !depth || !normal || !color || !params || !motion) return IRT_E_INVALID;
-    if (format < IRT_GBUFFER_F32 || format > IRT_GBUFFER_PACKED) return IRT_E_INVALID;
+// Flattened primitive table of a workload on the current device (static
+// scenes: built once and kept with the workload).
+cudaError_t irt_workload_prims(const irt_workload* wl_c, const void** prims_out, uint32_t* n_out) {
     irt_workload* wl = const_cast<irt_workload*>(wl_c);
     irt::Workload& w = wl->w;
     int dev = 0;
-    cudaGetDevice(&dev);
-    // Flattened primitive table (static scenes: built once per device).
-    std::vector<GPrim> prims;
-    for (uint32_t oi = 0; oi < w.objs.size(); oi++) {
-        const irt::Obj& ob = w.objs[oi];
-        irt_mat4 model = irt::to_f32(ob.model), inv = irt::to_f32(ob.inv_model);
-        const irt_material& m = w.materials[ob.material];
-        for (const irt::Part& part : w.mesh_desc[ob.mesh].parts) {
-            GPrim g{};
-            for (int k = 0; k < 16; k++) {
-                g.inv_model[k] = inv.m[k];
-                g.model[k] = model.m[k];
-            }
-            for (int a = 0; a < 3; a++) {
-                g.lo[a] = part.sphere ? 0.f : (float)part.lo[a];
-                g.hi[a] = part.sphere ? 0.f : (float)part.hi[a];
-            }
-            if (part.sphere) g.lo[0] = (float)part.radius;
-            for (int k = 0; k < 3; k++) g.color[k] = m.color[k];
-            g.params[0] = fminf(fmaxf(m.params[0], .045f), 1.f);
-            g.params[1] = fminf(fmaxf(m.params[1], 0.f), 1.f);
-            g.object = oi;
-            g.sphere = part.sphere ? 1u : 0u;
-            prims.push_back(g);
-        }
-    }
+    cudaError_t e = cudaGetDevice(&dev);
+    if (e != cudaSuccess) return e;
     if (!w.dev_prims || w.dev_prims_device != dev) {
+        std::vector<GPrim> prims;
+        for (uint32_t oi = 0; oi < w.objs.size(); oi++) {
+            const irt::Obj& ob = w.objs[oi];
+            irt_mat4 model = irt::to_f32(ob.model), inv = irt::to_f32(ob.inv_model);
+            const irt_material& m = w.materials[ob.material];
+            for (const irt::Part& part : w.mesh_desc[ob.mesh].parts) {
+                GPrim g{};
+                for (int k = 0; k < 16; k++) {
+                    g.inv_model[k] = inv.m[k];
+                    g.model[k] = model.m[k];
+                }
+                for (int a = 0; a < 3; a++) {
+                    g.lo[a] = part.sphere ? 0.f : (float)part.lo[a];
+                    g.hi[a] = part.sphere ? 0.f : (float)part.hi[a];
+                }
+                if (part.sphere) g.lo[0] = (float)part.radius;
+                for (int k = 0; k < 3; k++) g.color[k] = m.color[k];
+                g.params[0] = fminf(fmaxf(m.params[0], .045f), 1.f);
+                g.params[1] = fminf(fmaxf(m.params[1], 0.f), 1.f);
+                g.object = oi;
+                g.sphere = part.sphere ? 1u : 0u;
+                prims.push_back(g);
+            }
+        }
         if (w.dev_prims) cudaFree(w.dev_prims);
         w.dev_prims = nullptr;
-        if (cudaMalloc(&w.dev_prims, prims.size() * sizeof(GPrim)) != cudaSuccess) return IRT_E_CUDA;
-        if (cudaMemcpy(w.dev_prims, prims.data(), prims.size() * sizeof(GPrim), cudaMemcpyHostToDevice) != cudaSuccess)
-            return IRT_E_CUDA;
+        e = cudaMalloc(&w.dev_prims, prims.size() * sizeof(GPrim));
+        if (e != cudaSuccess) return e;
+        e = cudaMemcpy(w.dev_prims, prims.data(), prims.size() * sizeof(GPrim), cudaMemcpyHostToDevice);
+        if (e != cudaSuccess) return e;
         w.dev_prims_device = dev;
+        w.dev_prims_count = (uint32_t)prims.size();
     }
+    *prims_out = w.dev_prims;
+    *n_out = w.dev_prims_count;
+    return cudaSuccess;
+}
+
+extern "C" irt_status irt_gbuffer_render(irt_context* ctx, const irt_workload* wl, const irt_frame* f,
+                                         const irt_object* objects, int32_t format, float* depth, void* normal,
+                                         void* color, void* params, void* motion, void* stream) {
+    (void)objects;
+    if (!ctx || !wl || !f || !depth || !normal || !color || !params || !motion) return IRT_E_INVALID;
+    if (format < IRT_GBUFFER_F32 || format > IRT_GBUFFER_PACKED) return IRT_E_INVALID;
+    const void* prims = nullptr;
+    uint32_t n = 0;
+    if (irt_workload_prims(wl, &prims, &n) != cudaSuccess) return IRT_E_CUDA;
     dim3 block(32, 8);
     dim3 grid((f->size[0] + 31) / 32, (f->size[1] + 7) / 8);
     gbuffer_kernel<<<grid, block, 0, static_cast<cudaStream_t>(stream)>>>(
-        *f, static_cast<const GPrim*>(w.dev_prims), (uint32_t)prims.size(), format, depth, normal, color, params, motion);
+        *f, static_cast<const GPrim*>(prims), n, format, depth, normal, color, params, motion);
     return cudaGetLastError() == cudaSuccess ? IRT_OK : IRT_E_CUDA;
 }

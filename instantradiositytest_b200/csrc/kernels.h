@@ -114,6 +114,20 @@ struct SvgfLaunch {
 // of this frame (out = float4[W*H]), 4 guide of the previous frame (from
 // old_depth and previous_inv_vp).
 
+// VPL paths of one frame (vplgen.cu): lights on the device, ray casts
+// against a workload's analytic primitive table.
+struct VplLaunch {
+    const irt_frame* frame;
+    const void* prims;  // irt::GPrim[n_prims]
+    uint32_t n_prims;
+    const irt_light* lights;
+    irt_vpl* out;
+};
+cudaError_t irt_launch_vpls(const VplLaunch& L, cudaStream_t st);
+// The workload's flattened primitive table on the current device (built on
+// first use and kept with the workload).
+cudaError_t irt_workload_prims(const irt_workload* wl, const void** prims, uint32_t* n);
+
 cudaError_t irt_launch_lighting(const LightingLaunch& L, int stage, cudaStream_t st);
 // Lights with the spot direction normalised and cos(angle / 2) in
 // direction_angle, the form the lighting kernels read.

@@ -43,6 +43,7 @@ struct Workload {
     // producer (lazily created, owned here).
     void* dev_prims = nullptr;
     int dev_prims_device = -1;
+    uint32_t dev_prims_count = 0;
 
     bool build();
     void camera_at(uint32_t frame, double eye[3], double target[3]) const;
