@@ -392,6 +392,65 @@ irt_status irt_gbuffer_render(irt_context* ctx, const irt_workload* wl, const ir
 irt_status irt_vpl_generate(irt_scene* scene, const irt_workload* wl, const irt_frame* frame,
                             irt_vpl* out, void* stream);
 
+/* ---------------------------------------------------------------------------
+ * Render server: continuous batching of render sessions (no counterpart in
+ * the reference, which renders one view from one Renderer).
+ *
+ * Requests arrive over time (arrival_s, seconds after irt_server_run starts);
+ * each is a render session of `frames` frames over a synthetic workload (its
+ * scene, camera path and frame size).  The server admits waiting requests in
+ * arrival order while their HBM bytes (session history, scene, per-frame
+ * inputs) fit the server's budget and a slot is free; an admitted session
+ * keeps its reservoirs and SVGF history resident until its last frame and
+ * then frees them, so the next request can enter.  Admitted sessions are
+ * spread over CUDA streams and their frames interleave on the device: each
+ * frame is scene update, G-buffer, VPL generation and the lighting + SVGF
+ * hot path (irt_render_frame) on the session's stream.  Frames of a session
+ * are paced at frame_rate (0 = as fast as possible) with at most two in
+ * flight.  A session's results do not depend on what else runs with it.
+ * ------------------------------------------------------------------------- */
+typedef struct irt_server irt_server;
+
+typedef struct irt_server_desc {
+    uint64_t hbm_budget_bytes;  /* admission budget for all admitted sessions   */
+    uint32_t max_sessions;      /* admitted at once (0 = limited by bytes only) */
+    uint32_t streams;           /* CUDA streams sessions are spread over (>= 1) */
+    float frame_rate;           /* per-session pacing in frames/s; 0 = none     */
+    int32_t gbuffer_format, radiance_format, moments_format;
+    int32_t fused;              /* session schedule (irt_session_desc.fused)    */
+} irt_server_desc;
+
+typedef struct irt_request {
+    uint64_t id;
+    double arrival_s;           /* seconds after irt_server_run starts          */
+    uint32_t frames;
+    irt_workload* workload;     /* scene + camera path; caller-owned, outlives the run */
+    uint32_t capture_frame;     /* frame whose filtered image is copied ...     */
+    void* capture;              /* ... to this host buffer (NULL = none)        */
+} irt_request;
+
+typedef struct irt_server_stats {
+    uint64_t frames, sessions, rejected;
+    double pixel_frames;        /* sum of W*H over rendered frames              */
+    double seconds;             /* first admission to last completion           */
+    double mpix_frames_per_s;
+    float p50_latency_ms, p99_latency_ms;  /* frame due -> frame done            */
+    float p50_frame_ms, p99_frame_ms;      /* device time of a frame, start->end */
+    float p50_wait_ms, p99_wait_ms;        /* arrival -> admission               */
+    float mean_active, peak_active;
+    uint64_t peak_bytes;
+} irt_server_stats;
+
+irt_status irt_server_create(irt_context* ctx, const irt_server_desc* desc, irt_server** out);
+/* Queues a request (before or between runs).  A request whose bytes exceed
+ * the whole budget is rejected at run time and counted in stats.rejected. */
+irt_status irt_server_submit(irt_server* server, const irt_request* request);
+/* Serves every queued request to completion; host-blocking. */
+irt_status irt_server_run(irt_server* server, irt_server_stats* stats);
+/* HBM bytes the server charges a request against its budget. */
+uint64_t irt_server_request_bytes(const irt_server* server, const irt_request* request);
+void irt_server_destroy(irt_server* server);
+
 #ifdef __cplusplus
 }
 #endif

@@ -94,6 +94,35 @@ class WorkloadSpec(C.Structure):
     ]
 
 
+class ServerDesc(C.Structure):
+    _fields_ = [
+        ("hbm_budget_bytes", C.c_uint64), ("max_sessions", C.c_uint32), ("streams", C.c_uint32),
+        ("frame_rate", C.c_float), ("gbuffer_format", C.c_int32), ("radiance_format", C.c_int32),
+        ("moments_format", C.c_int32), ("fused", C.c_int32),
+    ]
+
+
+class Request(C.Structure):
+    _fields_ = [
+        ("id", C.c_uint64), ("arrival_s", C.c_double), ("frames", C.c_uint32), ("workload", C.c_void_p),
+        ("capture_frame", C.c_uint32), ("capture", C.c_void_p),
+    ]
+
+
+class ServerStats(C.Structure):
+    _fields_ = [
+        ("frames", C.c_uint64), ("sessions", C.c_uint64), ("rejected", C.c_uint64),
+        ("pixel_frames", C.c_double), ("seconds", C.c_double), ("mpix_frames_per_s", C.c_double),
+        ("p50_latency_ms", C.c_float), ("p99_latency_ms", C.c_float),
+        ("p50_frame_ms", C.c_float), ("p99_frame_ms", C.c_float),
+        ("p50_wait_ms", C.c_float), ("p99_wait_ms", C.c_float),
+        ("mean_active", C.c_float), ("peak_active", C.c_float), ("peak_bytes", C.c_uint64),
+    ]
+
+    def as_dict(self):
+        return {k: getattr(self, k) for k, _ in self._fields_}
+
+
 # numpy record layouts of the array-of-struct types (byte-identical to irt.h)
 OBJECT_DTYPE = np.dtype([("model", "<f4", 16), ("previous", "<f4", 16), ("inverse", "<f4", 16),
                          ("info", "<u4", 4)])
@@ -165,6 +194,11 @@ _PROTOS = {
     "irt_workload_vpls_cpu": (I32, [P, C.POINTER(Frame), P, P, P]),
     "irt_gbuffer_render": (I32, [P, P, C.POINTER(Frame), P, I32, P, P, P, P, P, P]),
     "irt_vpl_generate": (I32, [P, P, C.POINTER(Frame), P, P]),
+    "irt_server_create": (I32, [P, C.POINTER(ServerDesc), C.POINTER(P)]),
+    "irt_server_submit": (I32, [P, C.POINTER(Request)]),
+    "irt_server_run": (I32, [P, C.POINTER(ServerStats)]),
+    "irt_server_request_bytes": (U64, [P, C.POINTER(Request)]),
+    "irt_server_destroy": (None, [P]),
 }
 
 

@@ -382,7 +382,6 @@ bool Workload::build() {
     else
         atlas32.assign(texels, 0.f);
     meshes.resize(count);
-    mesh_samples.resize(count);
     for (uint32_t m = 0; m < count; m++) {
         MeshDesc& md = mesh_desc[m];
         for (const Part& p : md.parts) {
@@ -391,6 +390,13 @@ bool Workload::build() {
             else
                 box_mesh(p.lo, p.hi, md.vertices, md.indices);
         }
+    }
+    // Meshes are independent (each writes its own atlas tile): one thread
+    // per mesh samples its grid, derives its metadata and fills its tile.
+#pragma omp parallel for schedule(dynamic, 1)
+    for (int64_t mi = 0; mi < (int64_t)count; mi++) {
+        const uint32_t m = (uint32_t)mi;
+        MeshDesc& md = mesh_desc[m];
         // Exporter SDF conventions (tools/export_scene.py:136-152): padding of
         // two voxels of the vertex-box diagonal, bias of -extent * 2e-6.
         double lo[3] = {1e300, 1e300, 1e300}, hi[3] = {-1e300, -1e300, -1e300};
@@ -408,14 +414,12 @@ bool Workload::build() {
         }
         double ext = std::sqrt(std::pow(md.sdf_hi[0] - md.sdf_lo[0], 2) + std::pow(md.sdf_hi[1] - md.sdf_lo[1], 2) +
                                std::pow(md.sdf_hi[2] - md.sdf_lo[2], 2));
-        std::vector<float>& smp = mesh_samples[m];
-        smp.resize((size_t)res * res * res);
-#pragma omp parallel for schedule(static)
-        for (int64_t z = 0; z < (int64_t)res; z++)
+        std::vector<float> smp((size_t)res * res * res);
+        for (uint32_t z = 0; z < res; z++)
             for (uint32_t y = 0; y < res; y++)
                 for (uint32_t x = 0; x < res; x++) {
                     double p[3];
-                    uint32_t c[3] = {x, y, (uint32_t)z};
+                    uint32_t c[3] = {x, y, z};
                     for (int a = 0; a < 3; a++)
                         p[a] = md.sdf_lo[a] + ((double)md.sdf_hi[a] - md.sdf_lo[a]) * c[a] / (res - 1);
                     double d = 1e300;

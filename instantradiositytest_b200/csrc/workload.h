@@ -33,7 +33,6 @@ struct Workload {
     std::vector<irt_material> materials;
     std::vector<irt_light> lights;
     std::vector<irt_mesh> meshes;
-    std::vector<std::vector<float>> mesh_samples;
     std::vector<float> atlas32;
     std::vector<uint16_t> atlas16;
     uint32_t atlas_dims[3] = {0, 0, 0}, atlas_grid[3] = {0, 0, 0};

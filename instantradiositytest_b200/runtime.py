@@ -202,7 +202,7 @@ class FrameDriver:
 
     def __init__(self, wl: Workload, ctx: Context | None = None, gbuffer_format=L.GBUFFER_F32,
                  radiance_format=L.RADIANCE_F32, fused=True, keep_candidates=False, gpu_gbuffer=False,
-                 exact_march=False, moments_format=L.MOMENTS_F32):
+                 exact_march=False, moments_format=L.MOMENTS_F32, gpu_vpls=False):
         self.wl = wl
         self.ctx = ctx or Context()
         self.own_ctx = ctx is None
@@ -211,13 +211,14 @@ class FrameDriver:
         self.session = Session(self.ctx, session_desc(wl.settings, gbuffer_format, radiance_format, fused,
                                                       keep_candidates, exact_march, moments_format))
         self.gpu_gbuffer = gpu_gbuffer
+        self.gpu_vpls = gpu_vpls
         self.prev_vpls = None
         self.last = None
 
     def inputs(self, index: int, debug: int = 0):
         f, objects, nodes, lights = self.wl.frame(index, debug)
         planes = None if self.gpu_gbuffer else self.wl.gbuffer_cpu(f, self.fmt)
-        vpls = self.wl.vpls_cpu(f, objects, lights)
+        vpls = None if self.gpu_vpls else self.wl.vpls_cpu(f, objects, lights)
         return f, objects, nodes, lights, planes, vpls
 
     def step(self, index: int, debug: int = 0, inputs=None):
@@ -230,7 +231,12 @@ class FrameDriver:
             L.check(lib.irt_gbuffer_render(self.ctx.handle, self.wl.handle, C.byref(f), None, self.fmt,
                                            gs.depth, gs.normal, gs.color, gs.params, gs.motion, stream_handle()),
                     self.ctx.handle, "gbuffer render")
-        cur = vpls_to_device(vpls)
+        if vpls is None:
+            cur = torch.zeros(f.counts[1] * 48, dtype=torch.uint8, device="cuda")
+            L.check(lib.irt_vpl_generate(self.scene.handle, self.wl.handle, C.byref(f), C.c_void_p(cur.data_ptr()),
+                                         stream_handle()), self.ctx.handle, "vpl generate")
+        else:
+            cur = vpls_to_device(vpls)
         prev = self.prev_vpls if self.prev_vpls is not None else torch.zeros_like(cur)
         self.session.render(self.scene, f, gs, C.c_void_p(cur.data_ptr()), C.c_void_p(prev.data_ptr()))
         self.prev_vpls = cur
