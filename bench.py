@@ -110,7 +110,7 @@ def parse():
     ap.add_argument("--cpu-seconds", type=float, default=15.0, help="CPU work budget of the cpu_baseline sample")
     ap.add_argument("--reference-seconds", type=float, default=150.0, help="CPU budget of the reference arm")
     ap.add_argument("--serve-seconds", type=float, default=6.0, help="arrival window of the serving workload")
-    ap.add_argument("--serve-streams", type=int, default=8)
+    ap.add_argument("--serve-streams", type=int, default=2)
     return ap.parse_args()
 
 
