@@ -129,6 +129,36 @@ struct Sv {
     }
 };
 
+// Per-view record of a batched SVGF stage (the SvgfLaunch fields the stage
+// reads, with the context in kernel form).
+template <class G>
+struct SView {
+    SvgfCtx<G> c;
+    const void* in;
+    const void* aux;
+    const void* moments_in;
+    void* out;
+    void* out2;
+    void* moments_out;
+    int32_t step;
+};
+
+__device__ __forceinline__ uint32_t svgf_find_view(const uint32_t* __restrict__ start, uint32_t n, uint32_t b) {
+    uint32_t lo = 0, hi = n;
+    while (hi - lo > 1) {
+        uint32_t mid = (lo + hi) >> 1;
+        if (__ldg(start + mid) <= b) lo = mid;
+        else hi = mid;
+    }
+    return lo;
+}
+// Pixel of this thread in 2-D tile t of a view of width W.
+__device__ __forceinline__ void svgf_tile_xy(uint32_t W, uint32_t t, int32_t& x, int32_t& y) {
+    uint32_t tiles_x = (W + blockDim.x - 1) / blockDim.x;
+    x = (int32_t)((t % tiles_x) * blockDim.x + threadIdx.x);
+    y = (int32_t)((t / tiles_x) * blockDim.y + threadIdx.y);
+}
+
 // Calls fn(G{}, R{}, M{}) with the G-buffer, radiance and moment storage
 // types a launch names.
 template <class Fn>

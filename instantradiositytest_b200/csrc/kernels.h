@@ -11,6 +11,7 @@ constexpr int kStageReuse = 100;    // fused 0..3
 constexpr int kStageShade = 101;    // fused 4..7 with the march inline (one thread per pixel)
 constexpr int kStageSpatial = 102;  // fused 4..5 + resolve set-up: emits visibility rays
 constexpr int kStageCombine = 103;  // resolve 6..7 from contributions x visibility
+constexpr int kStageArchive = 104;  // batched: VPL archive slot copy + ray-counter reset
 
 // A visibility ray of the resolve passes (sdf.wgsl:61-81 arguments), 64 bytes:
 //   a = (p.xyz, bits(pixel * 2 + kind))  kind 0 = direct, 1 = indirect
@@ -129,6 +130,67 @@ cudaError_t irt_launch_vpls(const VplLaunch& L, cudaStream_t st);
 cudaError_t irt_workload_prims(const irt_workload* wl, const void** prims, uint32_t* n);
 
 cudaError_t irt_launch_lighting(const LightingLaunch& L, int stage, cudaStream_t st);
+
+// ------------------------------------------------------------------ batched views
+// One launch per pass over the views of a batch.  `table` is a device array
+// of n per-view argument records of the stage (lighting: the LightArgs of
+// irt_lighting_args_fill; SVGF: the records of irt_svgf_view_fill),
+// `frames` the n per-view frames on the device, `tile_start` n+1 block
+// offsets (2-D kernels: tiles of bx x by pixels; 1-D kernels: 256 pixels).
+struct BatchLaunch {
+    uint32_t n;
+    const irt_frame* frames;
+    const void* table;
+    const uint32_t* tile_start;
+    uint32_t tiles;
+    uint32_t bx, by;
+    int gbuffer_format;
+    int radiance_f16, moments_f16;
+    int keep;
+};
+size_t irt_lighting_args_size(int gbuffer_format);
+void irt_lighting_args_fill(const LightingLaunch& L, void* out);
+cudaError_t irt_launch_lighting_batched(const BatchLaunch& B, int stage, cudaStream_t st);
+// SVGF stages of a batch: 0 temporal, 1 variance, 2 a-trous (records carry
+// the step), 3 guides of this frame, 4 guides of the previous frame, 5 depth
+// and normal history copy.
+size_t irt_svgf_view_size(int gbuffer_format);
+void irt_svgf_view_fill(const SvgfLaunch& L, void* out);
+cudaError_t irt_launch_svgf_batched(const BatchLaunch& B, int stage, cudaStream_t st);
+cudaError_t irt_launch_svgf_spatial_batched(const BatchLaunch& B, int stage, cudaStream_t st);
+
+// Batched march: views grouped by scene; each group's compact scene is
+// staged in shared memory once per CTA and the group's ray queues (one per
+// view) are consumed in order.
+struct MarchQueue {
+    const RayRecord* rays;
+    uint32_t* counters;
+    float* vis;
+};
+struct alignas(16) MarchGroup {
+    irt_frame f;                // counts[3] and sdf[] of the group's views
+    const irt_object* objects;
+    const irt_mesh* meshes;
+    const irt_node* nodes;
+    cudaTextureObject_t atlas;
+    int sdf_f16;
+    uint32_t* error;
+    const float4* march_scene;
+    uint32_t scene_vec4;
+    const uint4* cells;
+    float grid_org[3], grid_inv[3];
+    uint32_t q_begin, q_end;    // the group's queues in the queue table
+};
+struct MarchBatch {
+    uint32_t n_groups;
+    const MarchGroup* groups;   // device
+    const MarchQueue* queues;   // device
+    uint32_t max_scene_bytes;
+    int num_sms;
+    int blocks_per_sm;          // 0 = occupancy maximum
+    int fast;
+};
+cudaError_t irt_launch_march_batched(const MarchBatch& M, cudaStream_t st);
 // Lights with the spot direction normalised and cos(angle / 2) in
 // direction_angle, the form the lighting kernels read.
 cudaError_t irt_launch_prepare_lights(const irt_light* lights, uint32_t n, irt_light* out, cudaStream_t st);

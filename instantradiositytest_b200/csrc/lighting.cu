@@ -255,10 +255,8 @@ __global__ void prepare_lights_kernel(const irt_light* lights, uint32_t n, irt_l
 
 // ---------------------------------------------------------------- fused kernels
 template <class G>
-__global__ void __launch_bounds__(256) reuse_kernel(const __grid_constant__ irt_frame f, const __grid_constant__ LightArgs<G> a,
-                                                    int keep_candidates) {
-    uint32_t x = blockIdx.x * blockDim.x + threadIdx.x;
-    uint32_t y = blockIdx.y * blockDim.y + threadIdx.y;
+__device__ __forceinline__ void reuse_body(const irt_frame& f, const LightArgs<G>& a, int keep_candidates, uint32_t x,
+                                           uint32_t y) {
     if (x >= f.size[0] || y >= f.size[1]) return;
     Px<G> px(f, a, x, y);
     bool ok = px.valid();
@@ -277,6 +275,12 @@ __global__ void __launch_bounds__(256) reuse_kernel(const __grid_constant__ irt_
     px.temporal_indirect(ri, hv, s, qx, qy);
     res_store(a.dres[1], px.id, rd);
     res_store(a.ires[1], px.id, ri);
+}
+
+template <class G>
+__global__ void __launch_bounds__(256) reuse_kernel(const __grid_constant__ irt_frame f, const __grid_constant__ LightArgs<G> a,
+                                                    int keep_candidates) {
+    reuse_body<G>(f, a, keep_candidates, blockIdx.x * blockDim.x + threadIdx.x, blockIdx.y * blockDim.y + threadIdx.y);
 }
 
 template <class G, class R>
@@ -305,10 +309,7 @@ __global__ void __launch_bounds__(256) shade_kernel(const __grid_constant__ irt_
 // (warp-aggregated: one atomic per warp).  Lanes of out-of-image pixels stay
 // in the warp until the append so every shuffle sees all 32 lanes.
 template <class G, class R>
-__global__ void __launch_bounds__(256) spatial_prep_kernel(const __grid_constant__ irt_frame f,
-                                                           const __grid_constant__ LightArgs<G> a) {
-    uint32_t x = blockIdx.x * blockDim.x + threadIdx.x;
-    uint32_t y = blockIdx.y * blockDim.y + threadIdx.y;
+__device__ __forceinline__ void spatial_prep_body(const irt_frame& f, const LightArgs<G>& a, uint32_t x, uint32_t y) {
     const bool in = x < f.size[0] && y < f.size[1];
     RayRecord ray[2];
     int n_rays = 0;
@@ -367,7 +368,8 @@ __global__ void __launch_bounds__(256) spatial_prep_kernel(const __grid_constant
     }
     // Warp-aggregated append.
     const unsigned full = 0xffffffffu;
-    const int lane = threadIdx.x & 31;
+    // lane within the warp for any 2-D block shape (warps take consecutive linear thread ids)
+    const int lane = (int)((threadIdx.y * blockDim.x + threadIdx.x) & 31u);
     int incl = n_rays;
 #pragma unroll
     for (int o = 1; o < 32; o <<= 1) {
@@ -382,12 +384,17 @@ __global__ void __launch_bounds__(256) spatial_prep_kernel(const __grid_constant
     for (int k = 0; k < n_rays; k++) a.rays[slot + k] = ray[k];
 }
 
+template <class G, class R>
+__global__ void __launch_bounds__(256) spatial_prep_kernel(const __grid_constant__ irt_frame f,
+                                                           const __grid_constant__ LightArgs<G> a) {
+    spatial_prep_body<G, R>(f, a, blockIdx.x * blockDim.x + threadIdx.x, blockIdx.y * blockDim.y + threadIdx.y);
+}
+
 // resolve_direct / resolve_indirect outputs from contribution x visibility:
 // direct = c_d * vis_d (or the debug colour), noisy = min(direct + c_i * vis_i, 65000).
 template <class R>
-__global__ void __launch_bounds__(256) combine_kernel(const __grid_constant__ irt_frame f, const float4* pending,
-                                                      const float* vis, float4* direct_out, void* noisy_out) {
-    size_t i = (size_t)blockIdx.x * blockDim.x + threadIdx.x;
+__device__ __forceinline__ void combine_body(const irt_frame& f, const float4* pending, const float* vis,
+                                             float4* direct_out, void* noisy_out, size_t i) {
     size_t P = (size_t)f.size[0] * f.size[1];
     if (i >= P) return;
     float4 pd = pending[i * 2], pi = pending[i * 2 + 1];
@@ -397,6 +404,12 @@ __global__ void __launch_bounds__(256) combine_kernel(const __grid_constant__ ir
     direct_out[i] = make_float4(result.x, result.y, result.z, 1.f);
     if (pi.w != 0.f) result = result + V3{pi.x * v.y, pi.y * v.y, pi.z * v.y};
     store_noisy<R>(noisy_out, i, result);
+}
+
+template <class R>
+__global__ void __launch_bounds__(256) combine_kernel(const __grid_constant__ irt_frame f, const float4* pending,
+                                                      const float* vis, float4* direct_out, void* noisy_out) {
+    combine_body<R>(f, pending, vis, direct_out, noisy_out, (size_t)blockIdx.x * blockDim.x + threadIdx.x);
 }
 
 // ---------------------------------------------------------------- plain kernels
@@ -438,6 +451,76 @@ __global__ void __launch_bounds__(256) pass_kernel(const __grid_constant__ irt_f
         V3 total = px.resolve_indirect(ok, s, res_load(a.ires[2], px.id), V3{d.x, d.y, d.z});
         store_noisy<R>(a.noisy_out, px.id, total);
     }
+}
+
+// ---------------------------------------------------------------- batched views
+// One launch covers every view of a batch: block b belongs to the view v
+// with tile_start[v] <= b < tile_start[v + 1]; its tile within the view
+// follows the view's width in blocks.  Frames and per-view arguments live
+// in device tables; the per-pixel code is the single-view kernels'.
+__device__ __forceinline__ uint32_t find_view(const uint32_t* __restrict__ start, uint32_t n, uint32_t b) {
+    uint32_t lo = 0, hi = n;
+    while (hi - lo > 1) {
+        uint32_t mid = (lo + hi) >> 1;
+        if (__ldg(start + mid) <= b) lo = mid;
+        else hi = mid;
+    }
+    return lo;
+}
+__device__ __forceinline__ void tile_xy(const irt_frame& f, uint32_t t, uint32_t& x, uint32_t& y) {
+    uint32_t tiles_x = (f.size[0] + blockDim.x - 1) / blockDim.x;
+    x = (t % tiles_x) * blockDim.x + threadIdx.x;
+    y = (t / tiles_x) * blockDim.y + threadIdx.y;
+}
+
+template <class G>
+__global__ void __launch_bounds__(256) reuse_batched(const irt_frame* __restrict__ frames, const LightArgs<G>* __restrict__ args,
+                                                     const uint32_t* __restrict__ tile_start, uint32_t n, int keep) {
+    const uint32_t v = find_view(tile_start, n, blockIdx.x);
+    const irt_frame& f = frames[v];
+    uint32_t x, y;
+    tile_xy(f, blockIdx.x - __ldg(tile_start + v), x, y);
+    reuse_body<G>(f, args[v], keep, x, y);
+}
+
+template <class G, class R>
+__global__ void __launch_bounds__(256) spatial_prep_batched(const irt_frame* __restrict__ frames,
+                                                            const LightArgs<G>* __restrict__ args,
+                                                            const uint32_t* __restrict__ tile_start, uint32_t n) {
+    const uint32_t v = find_view(tile_start, n, blockIdx.x);
+    const irt_frame& f = frames[v];
+    uint32_t x, y;
+    tile_xy(f, blockIdx.x - __ldg(tile_start + v), x, y);
+    spatial_prep_body<G, R>(f, args[v], x, y);
+}
+
+template <class G, class R>
+__global__ void __launch_bounds__(256) combine_batched(const irt_frame* __restrict__ frames,
+                                                       const LightArgs<G>* __restrict__ args,
+                                                       const uint32_t* __restrict__ tile_start, uint32_t n) {
+    const uint32_t v = find_view(tile_start, n, blockIdx.x);
+    const LightArgs<G>& a = args[v];
+    combine_body<R>(frames[v], a.pending, a.vis, a.direct_out, a.noisy_out,
+                    (size_t)(blockIdx.x - __ldg(tile_start + v)) * blockDim.x + threadIdx.x);
+}
+
+// VPL archive slot frame % (H+1) of every view, and the ray-queue counters
+// reset (src/renderer.rs:1873-1884).
+template <class G>
+__global__ void __launch_bounds__(256) archive_batched(const irt_frame* __restrict__ frames,
+                                                       const LightArgs<G>* __restrict__ args, uint32_t n) {
+    const uint32_t v = blockIdx.y;
+    if (v >= n) return;
+    const irt_frame& f = frames[v];
+    const LightArgs<G>& a = args[v];
+    const uint32_t count = f.counts[1];
+    const uint32_t slots = to_u32(f.rr[2]) + 1u;
+    const uint32_t slot = f.size[2] % slots;
+    const float4* src = reinterpret_cast<const float4*>(a.cur);
+    float4* dst = reinterpret_cast<float4*>(const_cast<irt_vpl*>(a.arch) + (size_t)slot * count);
+    for (uint32_t i = blockIdx.x * blockDim.x + threadIdx.x; i < count * 3u; i += gridDim.x * blockDim.x)
+        dst[i] = src[i];
+    if (blockIdx.x == 0 && threadIdx.x < 4) a.ray_counters[threadIdx.x] = 0u;
 }
 
 // ---------------------------------------------------------------- host launchers
@@ -503,7 +586,59 @@ static cudaError_t launch_typed(const LightingLaunch& L, int stage, cudaStream_t
     return cudaGetLastError();
 }
 
+template <class G, class R>
+static cudaError_t launch_batched_typed(const BatchLaunch& B, int stage, cudaStream_t st) {
+    const irt_frame* frames = B.frames;
+    const LightArgs<G>* args = static_cast<const LightArgs<G>*>(B.table);
+    dim3 block(B.bx, B.by);
+    switch (stage) {
+    case kStageReuse: reuse_batched<G><<<B.tiles, block, 0, st>>>(frames, args, B.tile_start, B.n, B.keep); break;
+    case kStageSpatial: spatial_prep_batched<G, R><<<B.tiles, block, 0, st>>>(frames, args, B.tile_start, B.n); break;
+    case kStageCombine: combine_batched<G, R><<<B.tiles, 256, 0, st>>>(frames, args, B.tile_start, B.n); break;
+    case kStageArchive: archive_batched<G><<<dim3(8, B.n), 256, 0, st>>>(frames, args, B.n); break;
+    default: return cudaErrorInvalidValue;
+    }
+    return cudaGetLastError();
+}
+
 }  // namespace irtd
+
+size_t irt_lighting_args_size(int gbuffer_format) {
+    using namespace irtd;
+    switch (gbuffer_format) {
+    case IRT_GBUFFER_F32: return sizeof(LightArgs<GbF32>);
+    case IRT_GBUFFER_F16: return sizeof(LightArgs<GbF16>);
+    default: return sizeof(LightArgs<GbPacked>);
+    }
+}
+
+void irt_lighting_args_fill(const LightingLaunch& L, void* out) {
+    using namespace irtd;
+    switch (L.gbuffer.format) {
+    case IRT_GBUFFER_F32: *static_cast<LightArgs<GbF32>*>(out) = make_args<GbF32>(L); break;
+    case IRT_GBUFFER_F16: *static_cast<LightArgs<GbF16>*>(out) = make_args<GbF16>(L); break;
+    default: *static_cast<LightArgs<GbPacked>*>(out) = make_args<GbPacked>(L); break;
+    }
+}
+
+cudaError_t irt_launch_lighting_batched(const BatchLaunch& B, int stage, cudaStream_t st) {
+    using namespace irtd;
+    if (B.n == 0) return cudaSuccess;
+    if (B.radiance_f16) {
+        switch (B.gbuffer_format) {
+        case IRT_GBUFFER_F32: return launch_batched_typed<GbF32, RadF16>(B, stage, st);
+        case IRT_GBUFFER_F16: return launch_batched_typed<GbF16, RadF16>(B, stage, st);
+        case IRT_GBUFFER_PACKED: return launch_batched_typed<GbPacked, RadF16>(B, stage, st);
+        }
+    } else {
+        switch (B.gbuffer_format) {
+        case IRT_GBUFFER_F32: return launch_batched_typed<GbF32, RadF32>(B, stage, st);
+        case IRT_GBUFFER_F16: return launch_batched_typed<GbF16, RadF32>(B, stage, st);
+        case IRT_GBUFFER_PACKED: return launch_batched_typed<GbPacked, RadF32>(B, stage, st);
+        }
+    }
+    return cudaErrorInvalidValue;
+}
 
 cudaError_t irt_launch_prepare_lights(const irt_light* lights, uint32_t n, irt_light* out, cudaStream_t st) {
     if (n == 0) return cudaSuccess;

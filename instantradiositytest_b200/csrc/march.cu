@@ -202,6 +202,131 @@ __global__ void __launch_bounds__(128, 6) march_kernel(const __grid_constant__ i
     }
 }
 
+// Batched march: for each scene group the CTA stages the group record and
+// its compact scene in shared memory, then its warps consume the group's ray
+// queues (one per view) in order with the same per-lane state machine; a
+// lane keeps the visibility array of the queue its ray came from.
+constexpr uint32_t kGroupVec4 = (uint32_t)((sizeof(MarchGroup) + 15) / 16);
+
+__global__ void __launch_bounds__(128, 6) march_batched_kernel(const MarchGroup* __restrict__ groups, uint32_t n_groups,
+                                                            const MarchQueue* __restrict__ queues) {
+    extern __shared__ float4 smem[];
+    const MarchGroup& G = *reinterpret_cast<const MarchGroup*>(smem);
+    float4* scene_smem = smem + kGroupVec4;
+    const unsigned full = 0xffffffffu;
+    const int lane = threadIdx.x & 31;
+    for (uint32_t g = 0; g < n_groups; g++) {
+        __syncthreads();  // every warp is done with the previous group's records
+        const float4* gsrc = reinterpret_cast<const float4*>(groups + g);
+        for (uint32_t i = threadIdx.x; i < kGroupVec4; i += blockDim.x) smem[i] = __ldg(gsrc + i);
+        __syncthreads();
+        for (uint32_t i = threadIdx.x; i < G.scene_vec4; i += blockDim.x) scene_smem[i] = __ldg(G.march_scene + i);
+        __syncthreads();
+        const irt_frame& f = G.f;
+        DevScene sc;
+        sc.objects = G.objects;
+        sc.meshes = G.meshes;
+        sc.nodes = G.nodes;
+        sc.lights = nullptr;
+        sc.atlas = G.atlas;
+        sc.sdf_f16 = G.sdf_f16;
+        sc.error = G.error;
+        Grid grid;
+        grid.cells = G.cells;
+        grid.ox = G.grid_org[0];
+        grid.oy = G.grid_org[1];
+        grid.oz = G.grid_org[2];
+        grid.ix = G.grid_inv[0];
+        grid.iy = G.grid_inv[1];
+        grid.iz = G.grid_inv[2];
+        const uint32_t n_obj = f.counts[3];
+        const MNode* nodes = reinterpret_cast<const MNode*>(scene_smem);
+        const MObj* objs = reinterpret_cast<const MObj*>(scene_smem + 2 * (2 * n_obj - 1));
+        const float eps = f.sdf[1];
+        const uint32_t max_steps = to_u32(f.sdf[0]);
+
+        uint32_t q = G.q_begin;
+        bool exhausted = q >= G.q_end;
+        uint32_t n_rays = exhausted ? 0u : *(volatile const uint32_t*)&queues[q].counters[0];
+        bool active = false;
+        uint32_t phase = kClear, slot = 0;
+        float* vis = nullptr;
+        MarchState m;
+        m.closest = kNone;
+        m.origin = V3{0.f, 0.f, 0.f};
+        m.dir = V3{0.f, 0.f, 0.f};
+        m.t = m.limit = 0.f;
+        m.result = 1.f;
+        m.previous = 1e20f;
+        m.step = 0;
+        V3 target{0.f, 0.f, 0.f}, endn{0.f, 0.f, 0.f};
+        for (;;) {
+            if (!exhausted) {
+                unsigned need = __ballot_sync(full, !active);
+                if (need) {
+                    const MarchQueue& Q = queues[q];
+                    int leader = __ffs(need) - 1;
+                    uint32_t cnt = (uint32_t)__popc(need);
+                    uint32_t base = 0;
+                    if (lane == leader) base = atomicAdd(&Q.counters[1], cnt);
+                    base = __shfl_sync(full, base, leader);
+                    if (!active) {
+                        uint32_t idx = base + (uint32_t)__popc(need & ((1u << lane) - 1u));
+                        if (idx < n_rays) {
+                            const float4* r = reinterpret_cast<const float4*>(Q.rays + idx);
+                            float4 a = __ldg(r), b = __ldg(r + 1), c = __ldg(r + 2), d = __ldg(r + 3);
+                            m.origin = V3{a.x, a.y, a.z};
+                            slot = __float_as_uint(a.w);
+                            m.dir = V3{b.x, b.y, b.z};
+                            target = V3{c.x, c.y, c.z};
+                            endn = V3{d.x, d.y, d.z};
+                            phase = kClear;
+                            vis = Q.vis;
+                            active = true;
+                        }
+                    }
+                    if (base + cnt >= n_rays) {  // this queue is used up: the next view's
+                        q++;
+                        if (q >= G.q_end) exhausted = true;
+                        else n_rays = *(volatile const uint32_t*)&queues[q].counters[0];
+                    }
+                }
+            }
+            if (!__any_sync(full, active)) {
+                if (exhausted) break;
+                continue;
+            }
+            if (!active) continue;
+
+            V3 qp = phase == kClear ? m.origin : (phase == kEndpoint ? target : march_point(m));
+            uint32_t hint = phase == kMarch ? m.closest : kNone;
+            Dist d = scene_distance_cached(sc, f, grid, nodes, objs, qp, hint, phase != kMarch);
+
+            float out = -1.f;
+            if (phase == kClear) {
+                m.closest = d.closest;
+                m.origin = m.origin + m.dir * clearance_epsilon(eps, d.voxel);
+                if (dot(endn, endn) > .5f) {
+                    phase = kEndpoint;
+                } else {
+                    phase = kMarch;
+                    out = march_begin(m, target, eps, max_steps);
+                }
+            } else if (phase == kEndpoint) {
+                phase = kMarch;
+                out = march_begin(m, target + endn * clearance_epsilon(eps, d.voxel), eps, max_steps);
+            } else {
+                m.closest = d.closest;
+                out = march_after(m, d.best, eps, f.sdf[2], max_steps);
+            }
+            if (out >= 0.f) {
+                vis[slot] = out;
+                active = false;
+            }
+        }
+    }
+}
+
 }  // namespace fast / exact
 }  // namespace irtd
 
@@ -252,7 +377,43 @@ cudaError_t IRT_MARCH_LAUNCH(const MarchLaunch& M, cudaStream_t st) {
     return cudaGetLastError();
 }
 
+#if IRT_MARCH_FAST
+#define IRT_MARCH_BATCHED_LAUNCH irt_launch_march_batched_fast
+#else
+#define IRT_MARCH_BATCHED_LAUNCH irt_launch_march_batched_exact
+#endif
+
+cudaError_t IRT_MARCH_BATCHED_LAUNCH(const MarchBatch& M, cudaStream_t st) {
+    using namespace irtd;
+    using namespace IRT_MARCH_NS;
+    if (M.n_groups == 0) return cudaSuccess;
+    const uint32_t smem = kGroupVec4 * 16 + M.max_scene_bytes;
+    thread_local int configured_device = -1;
+    thread_local uint32_t configured_smem = 0;
+    thread_local int max_blocks = 0;
+    int device = 0;
+    cudaGetDevice(&device);
+    if (smem != configured_smem || device != configured_device) {
+        configured_device = device;
+        cudaError_t e = cudaFuncSetAttribute(march_batched_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+        if (e != cudaSuccess) return e;
+        e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&max_blocks, march_batched_kernel, 128, smem);
+        if (e != cudaSuccess) return e;
+        if (max_blocks < 1) return cudaErrorInvalidConfiguration;
+        configured_smem = smem;
+    }
+    const int bps = M.blocks_per_sm > 0 && M.blocks_per_sm < max_blocks ? M.blocks_per_sm : max_blocks;
+    march_batched_kernel<<<M.num_sms * bps, 128, smem, st>>>(M.groups, M.n_groups, M.queues);
+    return cudaGetLastError();
+}
+
 #if !IRT_MARCH_FAST
+cudaError_t irt_launch_march_batched_fast(const MarchBatch& M, cudaStream_t st);
+
+cudaError_t irt_launch_march_batched(const MarchBatch& M, cudaStream_t st) {
+    return M.fast ? irt_launch_march_batched_fast(M, st) : irt_launch_march_batched_exact(M, st);
+}
+
 uint32_t irt_march_scene_bytes(uint32_t object_count) {
     return (2 * object_count - 1) * (uint32_t)sizeof(irtd::MNode) + object_count * (uint32_t)sizeof(irtd::MObj);
 }

@@ -18,12 +18,10 @@ namespace irtd {
 // (1-b)*var_h + b*(1-b)*(l - mean_h)^2), which equals the reference's
 // E[l^2] - E[l]^2 without its cancellation.
 template <class G, class R, class M>
-__global__ void __launch_bounds__(256) svgf_temporal_kernel(const __grid_constant__ irt_frame f, const __grid_constant__ SvgfCtx<G> c,
-                                                            const typename R::T* noisy, const typename R::T* old_radiance,
-                                                            const typename M::T* old_moments, typename R::T* radiance_out,
-                                                            typename M::T* moments_out) {
-    int32_t x = blockIdx.x * blockDim.x + threadIdx.x;
-    int32_t y = blockIdx.y * blockDim.y + threadIdx.y;
+__device__ __forceinline__ void temporal_body(const irt_frame& f, const SvgfCtx<G>& c, const typename R::T* noisy,
+                                              const typename R::T* old_radiance, const typename M::T* old_moments,
+                                              typename R::T* radiance_out, typename M::T* moments_out, int32_t x,
+                                              int32_t y) {
     Sv<G> sv(f, c);
     if (x >= sv.W || y >= sv.H) return;
     size_t i = sv.idx(x, y);
@@ -119,6 +117,29 @@ __global__ void __launch_bounds__(256) svgf_temporal_kernel(const __grid_constan
     M::store(moments_out, i, Moments{m0, M::central ? sqrtf(variance) : m1, age});
 }
 
+template <class G, class R, class M>
+__global__ void __launch_bounds__(256) svgf_temporal_kernel(const __grid_constant__ irt_frame f, const __grid_constant__ SvgfCtx<G> c,
+                                                            const typename R::T* noisy, const typename R::T* old_radiance,
+                                                            const typename M::T* old_moments, typename R::T* radiance_out,
+                                                            typename M::T* moments_out) {
+    temporal_body<G, R, M>(f, c, noisy, old_radiance, old_moments, radiance_out, moments_out,
+                           blockIdx.x * blockDim.x + threadIdx.x, blockIdx.y * blockDim.y + threadIdx.y);
+}
+
+template <class G, class R, class M>
+__global__ void __launch_bounds__(256) svgf_temporal_batched(const irt_frame* __restrict__ frames,
+                                                             const SView<G>* __restrict__ views,
+                                                             const uint32_t* __restrict__ tile_start, uint32_t n) {
+    const uint32_t v = svgf_find_view(tile_start, n, blockIdx.x);
+    const irt_frame& f = frames[v];
+    const SView<G>& w = views[v];
+    int32_t x, y;
+    svgf_tile_xy(f.size[0], blockIdx.x - __ldg(tile_start + v), x, y);
+    typedef typename R::T T;
+    temporal_body<G, R, M>(f, w.c, (const T*)w.in, (const T*)w.aux, (const typename M::T*)w.moments_in, (T*)w.out,
+                           (typename M::T*)w.moments_out, x, y);
+}
+
 // World position of every pixel, world(pixel_uv, depth, inv_vp)
 // (common.wgsl:46-47) with its f32 operations rounded one by one, and in w
 // the SVGF pixel scale distance(position, camera) / height (svgf.wgsl:30), or
@@ -126,9 +147,7 @@ __global__ void __launch_bounds__(256) svgf_temporal_kernel(const __grid_constan
 // here instead of recomputing them per neighbour tap.
 // With `previous` set, the same for the previous frame's depth and
 // previous_inv_vp (the positions history_valid / history_ok compare with).
-__global__ void __launch_bounds__(256) guide_kernel(const __grid_constant__ irt_frame f, const float* depth,
-                                                    int previous, float4* out) {
-    size_t i = (size_t)blockIdx.x * blockDim.x + threadIdx.x;
+__device__ __forceinline__ void guide_body(const irt_frame& f, const float* depth, int previous, float4* out, size_t i) {
     const uint32_t W = f.size[0];
     if (i >= (size_t)W * f.size[1]) return;
     uint32_t x = (uint32_t)(i % W), y = (uint32_t)(i / W);
@@ -137,6 +156,36 @@ __global__ void __launch_bounds__(256) guide_kernel(const __grid_constant__ irt_
                  previous ? f.previous_inv_vp : f.inv_vp);
     float s = d < 1.f ? distance(p, V3{f.camera[0], f.camera[1], f.camera[2]}) / (float)f.size[1] : -1.f;
     out[i] = make_float4(p.x, p.y, p.z, s);
+}
+
+__global__ void __launch_bounds__(256) guide_kernel(const __grid_constant__ irt_frame f, const float* depth,
+                                                    int previous, float4* out) {
+    guide_body(f, depth, previous, out, (size_t)blockIdx.x * blockDim.x + threadIdx.x);
+}
+
+// Batched guides (in = depth, out = guide) and depth/normal history copy
+// (in = depth, aux = normal, out = previous depth, out2 = previous normal);
+// 1-D tiles of 256 pixels.
+template <class G>
+__global__ void __launch_bounds__(256) guide_batched(const irt_frame* __restrict__ frames, const SView<G>* __restrict__ views,
+                                                     const uint32_t* __restrict__ tile_start, uint32_t n, int previous) {
+    const uint32_t v = svgf_find_view(tile_start, n, blockIdx.x);
+    const SView<G>& w = views[v];
+    guide_body(frames[v], (const float*)w.in, previous, (float4*)w.out,
+               (size_t)(blockIdx.x - __ldg(tile_start + v)) * blockDim.x + threadIdx.x);
+}
+
+template <class G>
+__global__ void __launch_bounds__(256) history_batched(const irt_frame* __restrict__ frames, const SView<G>* __restrict__ views,
+                                                       const uint32_t* __restrict__ tile_start, uint32_t n) {
+    const uint32_t v = svgf_find_view(tile_start, n, blockIdx.x);
+    const SView<G>& w = views[v];
+    const irt_frame& f = frames[v];
+    const size_t i = (size_t)(blockIdx.x - __ldg(tile_start + v)) * blockDim.x + threadIdx.x;
+    if (i >= (size_t)f.size[0] * f.size[1]) return;
+    ((float*)w.out)[i] = ((const float*)w.in)[i];
+    typedef typename G::NormalT N;
+    ((N*)w.out2)[i] = ((const N*)w.aux)[i];
 }
 
 template <class G, class R, class M>
@@ -163,7 +212,66 @@ static cudaError_t svgf_typed(const SvgfLaunch& L, int stage, cudaStream_t st) {
     return cudaGetLastError();
 }
 
+template <class G, class R, class M>
+static cudaError_t svgf_batched_typed(const BatchLaunch& B, int stage, cudaStream_t st) {
+    const SView<G>* views = static_cast<const SView<G>*>(B.table);
+    switch (stage) {
+    case 0: svgf_temporal_batched<G, R, M><<<B.tiles, dim3(B.bx, B.by), 0, st>>>(B.frames, views, B.tile_start, B.n); break;
+    case 3:
+    case 4: guide_batched<G><<<B.tiles, 256, 0, st>>>(B.frames, views, B.tile_start, B.n, stage == 4); break;
+    case 5: history_batched<G><<<B.tiles, 256, 0, st>>>(B.frames, views, B.tile_start, B.n); break;
+    default: return cudaErrorInvalidValue;
+    }
+    return cudaGetLastError();
+}
+
 }  // namespace irtd
+
+size_t irt_svgf_view_size(int gbuffer_format) {
+    using namespace irtd;
+    switch (gbuffer_format) {
+    case IRT_GBUFFER_F32: return sizeof(SView<GbF32>);
+    case IRT_GBUFFER_F16: return sizeof(SView<GbF16>);
+    default: return sizeof(SView<GbPacked>);
+    }
+}
+
+template <class G>
+static void fill_view(const SvgfLaunch& L, void* out) {
+    using namespace irtd;
+    SView<G> w;
+    w.c = make_ctx<G>(L);
+    w.in = L.in;
+    w.aux = L.aux;
+    w.moments_in = L.moments_in;
+    w.out = L.out;
+    w.out2 = L.out2;
+    w.moments_out = L.moments_out;
+    w.step = L.step;
+    *static_cast<SView<G>*>(out) = w;
+}
+
+void irt_svgf_view_fill(const SvgfLaunch& L, void* out) {
+    using namespace irtd;
+    switch (L.gbuffer.format) {
+    case IRT_GBUFFER_F32: fill_view<GbF32>(L, out); break;
+    case IRT_GBUFFER_F16: fill_view<GbF16>(L, out); break;
+    default: fill_view<GbPacked>(L, out); break;
+    }
+}
+
+cudaError_t irt_launch_svgf_batched(const BatchLaunch& B, int stage, cudaStream_t st) {
+    using namespace irtd;
+    if (B.n == 0) return cudaSuccess;
+    if (stage == 1 || stage == 2) return irt_launch_svgf_spatial_batched(B, stage, st);
+    SvgfLaunch L{};
+    L.gbuffer.format = B.gbuffer_format;
+    L.radiance_f16 = B.radiance_f16;
+    L.moments_f16 = B.moments_f16;
+    return dispatch_svgf(L, [&](auto g, auto r, auto m) {
+        return svgf_batched_typed<decltype(g), decltype(r), decltype(m)>(B, stage, st);
+    });
+}
 
 cudaError_t irt_launch_svgf(const SvgfLaunch& L, int stage, cudaStream_t st) {
     using namespace irtd;

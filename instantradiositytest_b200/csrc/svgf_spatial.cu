@@ -16,11 +16,8 @@ namespace irtd {
 // centre pixel's mean (shifted data), so E[l^2] - E[l]^2 is formed from
 // small numbers: s0 = sum w (m - K), s1 = sum w (dev^2 + (m - K)^2).
 template <class G, class R, class M>
-__global__ void __launch_bounds__(256) svgf_variance_kernel(const __grid_constant__ irt_frame f, const __grid_constant__ SvgfCtx<G> c,
-                                                            const typename R::T* input, const typename M::T* moments,
-                                                            typename R::T* out) {
-    int32_t x = blockIdx.x * blockDim.x + threadIdx.x;
-    int32_t y = blockIdx.y * blockDim.y + threadIdx.y;
+__device__ __forceinline__ void variance_body(const irt_frame& f, const SvgfCtx<G>& c, const typename R::T* input,
+                                              const typename M::T* moments, typename R::T* out, int32_t x, int32_t y) {
     Sv<G> sv(f, c);
     if (x >= sv.W || y >= sv.H) return;
     size_t i = sv.idx(x, y);
@@ -56,6 +53,14 @@ __global__ void __launch_bounds__(256) svgf_variance_kernel(const __grid_constan
     R::store(out, i, make_float4(in.x, in.y, in.z, wmin(sigma, 65000.f)));
 }
 
+template <class G, class R, class M>
+__global__ void __launch_bounds__(256) svgf_variance_kernel(const __grid_constant__ irt_frame f, const __grid_constant__ SvgfCtx<G> c,
+                                                            const typename R::T* input, const typename M::T* moments,
+                                                            typename R::T* out) {
+    variance_body<G, R, M>(f, c, input, moments, out, blockIdx.x * blockDim.x + threadIdx.x,
+                           blockIdx.y * blockDim.y + threadIdx.y);
+}
+
 __device__ __forceinline__ float wavelet_kernel(int32_t x) {
     if (x == 0) return 1.f;
     if (x == 1 || x == -1) return 2.f / 3.f;
@@ -64,11 +69,9 @@ __device__ __forceinline__ float wavelet_kernel(int32_t x) {
 
 // svgf.wgsl:91-110; `out2` (optional) receives a second copy of the result.
 template <class G, class R>
-__global__ void __launch_bounds__(256) svgf_atrous_kernel(const __grid_constant__ irt_frame f, const __grid_constant__ SvgfCtx<G> c,
-                                                          const typename R::T* input, typename R::T* out,
-                                                          typename R::T* out2, int32_t step) {
-    int32_t x = blockIdx.x * blockDim.x + threadIdx.x;
-    int32_t y = blockIdx.y * blockDim.y + threadIdx.y;
+__device__ __forceinline__ void atrous_body(const irt_frame& f, const SvgfCtx<G>& c, const typename R::T* input,
+                                            typename R::T* out, typename R::T* out2, int32_t step, int32_t x,
+                                            int32_t y) {
     Sv<G> sv(f, c);
     if (x >= sv.W || y >= sv.H) return;
     size_t i = sv.idx(x, y);
@@ -113,6 +116,40 @@ __global__ void __launch_bounds__(256) svgf_atrous_kernel(const __grid_constant_
     if (out2) R::store(out2, i, o);
 }
 
+template <class G, class R>
+__global__ void __launch_bounds__(256) svgf_atrous_kernel(const __grid_constant__ irt_frame f, const __grid_constant__ SvgfCtx<G> c,
+                                                          const typename R::T* input, typename R::T* out,
+                                                          typename R::T* out2, int32_t step) {
+    atrous_body<G, R>(f, c, input, out, out2, step, blockIdx.x * blockDim.x + threadIdx.x,
+                      blockIdx.y * blockDim.y + threadIdx.y);
+}
+
+template <class G, class R, class M>
+__global__ void __launch_bounds__(256) svgf_variance_batched(const irt_frame* __restrict__ frames,
+                                                             const SView<G>* __restrict__ views,
+                                                             const uint32_t* __restrict__ tile_start, uint32_t n) {
+    const uint32_t v = svgf_find_view(tile_start, n, blockIdx.x);
+    const irt_frame& f = frames[v];
+    const SView<G>& w = views[v];
+    int32_t x, y;
+    svgf_tile_xy(f.size[0], blockIdx.x - __ldg(tile_start + v), x, y);
+    typedef typename R::T T;
+    variance_body<G, R, M>(f, w.c, (const T*)w.in, (const typename M::T*)w.moments_in, (T*)w.out, x, y);
+}
+
+template <class G, class R>
+__global__ void __launch_bounds__(256) svgf_atrous_batched(const irt_frame* __restrict__ frames,
+                                                           const SView<G>* __restrict__ views,
+                                                           const uint32_t* __restrict__ tile_start, uint32_t n) {
+    const uint32_t v = svgf_find_view(tile_start, n, blockIdx.x);
+    const irt_frame& f = frames[v];
+    const SView<G>& w = views[v];
+    int32_t x, y;
+    svgf_tile_xy(f.size[0], blockIdx.x - __ldg(tile_start + v), x, y);
+    typedef typename R::T T;
+    atrous_body<G, R>(f, w.c, (const T*)w.in, (T*)w.out, (T*)w.out2, w.step, x, y);
+}
+
 template <class G, class R, class M>
 static cudaError_t spatial_typed(const SvgfLaunch& L, int stage, cudaStream_t st) {
     SvgfCtx<G> c = make_ctx<G>(L);
@@ -130,7 +167,31 @@ static cudaError_t spatial_typed(const SvgfLaunch& L, int stage, cudaStream_t st
     return cudaGetLastError();
 }
 
+template <class G, class R, class M>
+static cudaError_t spatial_batched_typed(const BatchLaunch& B, int stage, cudaStream_t st) {
+    const SView<G>* views = static_cast<const SView<G>*>(B.table);
+    dim3 block(B.bx, B.by);
+    if (stage == 1)
+        svgf_variance_batched<G, R, M><<<B.tiles, block, 0, st>>>(B.frames, views, B.tile_start, B.n);
+    else if (stage == 2)
+        svgf_atrous_batched<G, R><<<B.tiles, block, 0, st>>>(B.frames, views, B.tile_start, B.n);
+    else
+        return cudaErrorInvalidValue;
+    return cudaGetLastError();
+}
+
 }  // namespace irtd
+
+cudaError_t irt_launch_svgf_spatial_batched(const BatchLaunch& B, int stage, cudaStream_t st) {
+    using namespace irtd;
+    SvgfLaunch L{};
+    L.gbuffer.format = B.gbuffer_format;
+    L.radiance_f16 = B.radiance_f16;
+    L.moments_f16 = stage == 2 ? 0 : B.moments_f16;
+    return dispatch_svgf(L, [&](auto g, auto r, auto m) {
+        return spatial_batched_typed<decltype(g), decltype(r), decltype(m)>(B, stage, st);
+    });
+}
 
 cudaError_t irt_launch_svgf_spatial(const SvgfLaunch& L, int stage, cudaStream_t st) {
     using namespace irtd;
