@@ -393,6 +393,55 @@ irt_status irt_vpl_generate(irt_scene* scene, const irt_workload* wl, const irt_
                             irt_vpl* out, void* stream);
 
 /* ---------------------------------------------------------------------------
+ * Batched views (no counterpart in the reference, which renders one view per
+ * Renderer).  A batch renders many views of uneven size — each a session of
+ * its own with its own history, over its own scene or one shared with other
+ * views — with ONE launch per pass for all of them: per pass a tile table
+ * maps blocks to (view, tile) and per-view argument tables live on the
+ * device; the march is one persistent launch whose CTAs stage each scene's
+ * compact records in shared memory once and consume every view's ray queue
+ * of that scene.  With use_graphs, each frame's launches (frame upload
+ * included) are captured once per frame parity as a CUDA graph and replayed.
+ * Tile shapes come from the batch's autotuner (irt_batch_autotune).  Every
+ * view's results are those of irt_render_frame on that view alone.
+ * All views of a batch render the same frame index each call; debug views
+ * (frame.flags[2] != 0) are not batched.
+ * ------------------------------------------------------------------------- */
+typedef struct irt_batch irt_batch;
+
+typedef struct irt_batch_desc {
+    irt_settings settings;      /* shared by all views; render_width/height ignored */
+    int32_t gbuffer_format, radiance_format, moments_format;
+    int32_t use_graphs;         /* 1 = capture and replay a CUDA graph per frame     */
+    uint32_t n_views;
+    const uint32_t* widths;     /* n_views entries                                   */
+    const uint32_t* heights;    /* n_views entries                                   */
+} irt_batch_desc;
+
+irt_status irt_batch_create(irt_context* ctx, const irt_batch_desc* desc, irt_batch** out);
+/* One frame of every view: scenes[v] (already updated for this frame with
+ * irt_scene_update on the same stream), frames[v], gbuffers[v], current and
+ * previous VPL pools of view v.  The batch runs on a stream of its own that
+ * waits for `stream` and that `stream` then waits for. */
+irt_status irt_batch_render(irt_batch* b, irt_scene* const* scenes, const irt_frame* frames,
+                            const irt_gbuffer* gbuffers, const irt_vpl* const* current,
+                            const irt_vpl* const* previous, void* stream);
+/* The session that holds view v's history and outputs (irt_session_buffer). */
+irt_session* irt_batch_view(irt_batch* b, uint32_t view);
+/* The next `frames` calls of irt_batch_render (at least 5) try the candidate
+ * tile shapes (2-D kernels: 32x8, 64x4, 16x16, 128x2, 256x1; march CTAs per
+ * SM) and time every pass; afterwards each pass keeps its fastest shape. */
+irt_status irt_batch_autotune(irt_batch* b, uint32_t frames);
+/* The tile shapes in use, as text ("reuse=32x8 spatial=64x4 ... march=6"). */
+irt_status irt_batch_tuning(const irt_batch* b, char* out, size_t len);
+/* Device time of the last directly launched frame's passes (ms), 12 values:
+ * guides, archive, reuse, spatial, march, combine, temporal, variance,
+ * a-trous (all iterations), history, total, and 1 if the last frame was a
+ * graph replay (0 otherwise). */
+irt_status irt_batch_pass_ms(irt_batch* b, float* out12);
+void irt_batch_destroy(irt_batch* b);
+
+/* ---------------------------------------------------------------------------
  * Render server: continuous batching of render sessions (no counterpart in
  * the reference, which renders one view from one Renderer).
  *

@@ -94,6 +94,14 @@ class WorkloadSpec(C.Structure):
     ]
 
 
+class BatchDesc(C.Structure):
+    _fields_ = [
+        ("settings", Settings), ("gbuffer_format", C.c_int32), ("radiance_format", C.c_int32),
+        ("moments_format", C.c_int32), ("use_graphs", C.c_int32), ("n_views", C.c_uint32),
+        ("widths", C.POINTER(C.c_uint32)), ("heights", C.POINTER(C.c_uint32)),
+    ]
+
+
 class ServerDesc(C.Structure):
     _fields_ = [
         ("hbm_budget_bytes", C.c_uint64), ("max_sessions", C.c_uint32), ("streams", C.c_uint32),
@@ -194,6 +202,13 @@ _PROTOS = {
     "irt_workload_vpls_cpu": (I32, [P, C.POINTER(Frame), P, P, P]),
     "irt_gbuffer_render": (I32, [P, P, C.POINTER(Frame), P, I32, P, P, P, P, P, P]),
     "irt_vpl_generate": (I32, [P, P, C.POINTER(Frame), P, P]),
+    "irt_batch_create": (I32, [P, C.POINTER(BatchDesc), C.POINTER(P)]),
+    "irt_batch_render": (I32, [P, P, C.POINTER(Frame), C.POINTER(GBuffer), P, P, P]),
+    "irt_batch_view": (P, [P, U32]),
+    "irt_batch_autotune": (I32, [P, U32]),
+    "irt_batch_tuning": (I32, [P, C.c_char_p, C.c_size_t]),
+    "irt_batch_pass_ms": (I32, [P, C.POINTER(C.c_float)]),
+    "irt_batch_destroy": (None, [P]),
     "irt_server_create": (I32, [P, C.POINTER(ServerDesc), C.POINTER(P)]),
     "irt_server_submit": (I32, [P, C.POINTER(Request)]),
     "irt_server_run": (I32, [P, C.POINTER(ServerStats)]),

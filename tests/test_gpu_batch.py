@@ -1,0 +1,84 @@
+"""Batched views (irt_batch_*): every view of a batch — views of uneven size,
+some sharing a scene — gives exactly the results of rendering it alone with
+irt_render_frame, through the autotuner's candidate shapes, direct launches
+and CUDA-graph replays."""
+import ctypes as C
+
+import numpy as np
+import pytest
+import torch
+
+from instantradiositytest_b200 import _lib as L
+from instantradiositytest_b200.batching import BatchDriver
+from instantradiositytest_b200.runtime import Context, Scene, Session, gbuffer_device_alloc, session_desc, stream_handle
+from instantradiositytest_b200.workload import Workload, preset_spec
+
+pytestmark = pytest.mark.gpu
+
+BUFS = (L.BUF_DIRECT, L.BUF_NOISY, L.BUF_TEMPORAL, L.BUF_VARIANCE, L.BUF_MOMENTS, L.BUF_FEEDBACK, L.BUF_FILTERED,
+        L.BUF_PREV_DEPTH)
+
+
+def workload(seed, meshes, w, h):
+    return Workload(preset_spec(2, seed=seed, width=w, height=h, n_boxes=(meshes - 1) * 6 // 10,
+                                n_spheres=(meshes - 1) - (meshes - 1) * 6 // 10))
+
+
+def render_alone(ctx, wl, frames, fmt, rfmt, mfmt):
+    """One session over `frames` (the batch's frames of the view)."""
+    scene = Scene(ctx, wl.meshes, wl.atlas, wl.sdf_format)
+    sess = Session(ctx, session_desc(wl.settings, fmt, rfmt, 1, False, False, mfmt))
+    _, gs = gbuffer_device_alloc(wl.height, wl.width, fmt)
+    pools = [torch.zeros(wl.settings.vpl_count * 48, dtype=torch.uint8, device="cuda") for _ in range(3)]
+    sh = stream_handle()
+    for i, (f, obj, nodes, lights) in enumerate(frames):
+        scene.update(obj, nodes, lights)
+        L.check(L.lib.irt_gbuffer_render(ctx.handle, wl.handle, C.byref(f), None, fmt, gs.depth, gs.normal, gs.color,
+                                         gs.params, gs.motion, sh), ctx.handle, "gbuffer")
+        cur = pools[i % 2]
+        L.check(L.lib.irt_vpl_generate(scene.handle, wl.handle, C.byref(f), C.c_void_p(cur.data_ptr()), sh),
+                ctx.handle, "vpls")
+        prev = pools[(i + 1) % 2] if i > 0 else pools[2]
+        sess.render(scene, f, gs, C.c_void_p(cur.data_ptr()), C.c_void_p(prev.data_ptr()))
+    torch.cuda.synchronize()
+    out = {w: sess.buffer(w, torch.uint8).cpu().numpy() for w in BUFS}
+    out["res"] = [sess.reservoirs_host(d, 2).view(np.uint8) for d in (0, 1)]
+    sess.close()
+    scene.close()
+    return out
+
+
+@pytest.mark.parametrize("formats", [(L.GBUFFER_F32, L.RADIANCE_F32, L.MOMENTS_F32),
+                                     (L.GBUFFER_PACKED, L.RADIANCE_F16, L.MOMENTS_F16)])
+def test_batch_views_equal_alone(cuda, formats):
+    fmt, rfmt, mfmt = formats
+    a = workload(21, 12, 160, 100)
+    b = workload(22, 20, 224, 140)
+    c = workload(23, 8, 96, 64)
+    views = [(a, 0), (b, 0), (a, 7), (c, 2), (b, 11)]
+    ctx = Context()
+    drv = BatchDriver(ctx, views, fmt, rfmt, mfmt, use_graphs=True)
+    drv.batch.autotune(5)
+    n_frames = 12
+    per_view = [[] for _ in views]
+    for i in range(n_frames):
+        data = drv.inputs(i)
+        frames = drv.step(i, data)
+        for v, (f, (_, obj, nodes, lights)) in enumerate(zip(frames, data)):
+            per_view[v].append((L.Frame.from_buffer_copy(f), obj, nodes, lights))
+        if i == 6:
+            print("passes", drv.batch.pass_ms())
+    torch.cuda.synchronize()
+    print("tuning:", drv.batch.tuning())
+    assert drv.batch.pass_ms()["graph"] == 1.0  # the last frames were graph replays
+    for v, (wl, _) in enumerate(views):
+        s = drv.batch.view(v)
+        got = {w: s.buffer(w, torch.uint8).cpu().numpy() for w in BUFS}
+        ref = render_alone(ctx, wl, per_view[v], fmt, rfmt, mfmt)
+        for w in BUFS:
+            assert np.array_equal(got[w], ref[w]), (v, w)
+        for d in (0, 1):
+            assert np.array_equal(s.reservoirs_host(d, 2).view(np.uint8), ref["res"][d]), (v, d)
+        assert np.abs(got[L.BUF_DIRECT].view(np.float32)).max() > 0
+    drv.close()
+    ctx.close()
