@@ -416,6 +416,7 @@ typedef struct irt_batch_desc {
     uint32_t n_views;
     const uint32_t* widths;     /* n_views entries                                   */
     const uint32_t* heights;    /* n_views entries                                   */
+    const uint32_t* vpl_counts; /* n_views entries, or NULL = settings.vpl_count     */
 } irt_batch_desc;
 
 irt_status irt_batch_create(irt_context* ctx, const irt_batch_desc* desc, irt_batch** out);
@@ -428,11 +429,19 @@ irt_status irt_batch_render(irt_batch* b, irt_scene* const* scenes, const irt_fr
                             const irt_vpl* const* previous, void* stream);
 /* The session that holds view v's history and outputs (irt_session_buffer). */
 irt_session* irt_batch_view(irt_batch* b, uint32_t view);
-/* The next `frames` calls of irt_batch_render (at least 5) try the candidate
- * tile shapes (2-D kernels: 32x8, 64x4, 16x16, 128x2, 256x1; march CTAs per
- * SM) and time every pass; afterwards each pass keeps its fastest shape. */
+/* The next max(frames, 5) calls of irt_batch_render try the candidate tile
+ * shapes (2-D kernels: 32x8, 64x4, 16x16, 128x2, 256x1; march CTAs per SM)
+ * on one wave and time every pass, each pass keeping its fastest shape; the
+ * 5 calls after them time the frame at each wave budget and keep the
+ * fastest. */
 irt_status irt_batch_autotune(irt_batch* b, uint32_t frames);
-/* The tile shapes in use, as text ("reuse=32x8 spatial=64x4 ... march=6"). */
+/* Views run in waves: consecutive views whose pixels add up to at most
+ * budget_px share one launch per pass, wave after wave, so a wave's buffers
+ * stay in L2 between its passes (0 = all views in one wave).  The autotuner
+ * also picks it, among 0, 8, 4, 2 and 1 Mi pixels. */
+irt_status irt_batch_set_waves(irt_batch* b, uint64_t budget_px);
+/* The tile shapes and waves in use, as text
+ * ("reuse=32x8 ... march_ctas_per_sm=max waves=3 wave_budget_px=4194304"). */
 irt_status irt_batch_tuning(const irt_batch* b, char* out, size_t len);
 /* Device time of the last directly launched frame's passes (ms), 12 values:
  * guides, archive, reuse, spatial, march, combine, temporal, variance,

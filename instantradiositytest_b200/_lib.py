@@ -99,6 +99,7 @@ class BatchDesc(C.Structure):
         ("settings", Settings), ("gbuffer_format", C.c_int32), ("radiance_format", C.c_int32),
         ("moments_format", C.c_int32), ("use_graphs", C.c_int32), ("n_views", C.c_uint32),
         ("widths", C.POINTER(C.c_uint32)), ("heights", C.POINTER(C.c_uint32)),
+        ("vpl_counts", C.POINTER(C.c_uint32)),
     ]
 
 
@@ -207,6 +208,7 @@ _PROTOS = {
     "irt_batch_view": (P, [P, U32]),
     "irt_batch_autotune": (I32, [P, U32]),
     "irt_batch_tuning": (I32, [P, C.c_char_p, C.c_size_t]),
+    "irt_batch_set_waves": (I32, [P, U64]),
     "irt_batch_pass_ms": (I32, [P, C.POINTER(C.c_float)]),
     "irt_batch_destroy": (None, [P]),
     "irt_server_create": (I32, [P, C.POINTER(ServerDesc), C.POINTER(P)]),

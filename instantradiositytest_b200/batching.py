@@ -17,13 +17,15 @@ class Batch:
               "history", "total", "graph")
 
     def __init__(self, ctx: Context, settings: L.Settings, sizes, gbuffer_format=L.GBUFFER_F32,
-                 radiance_format=L.RADIANCE_F32, moments_format=L.MOMENTS_F32, use_graphs=True):
+                 radiance_format=L.RADIANCE_F32, moments_format=L.MOMENTS_F32, use_graphs=True, vpl_counts=None):
         self.ctx = ctx
         self.n = len(sizes)
         self._w = (C.c_uint32 * self.n)(*[w for w, _ in sizes])
         self._h = (C.c_uint32 * self.n)(*[h for _, h in sizes])
+        self._v = (C.c_uint32 * self.n)(*vpl_counts) if vpl_counts is not None else None
         self.desc = L.BatchDesc(settings, gbuffer_format, radiance_format, moments_format, int(use_graphs), self.n,
-                                C.cast(self._w, C.POINTER(C.c_uint32)), C.cast(self._h, C.POINTER(C.c_uint32)))
+                                C.cast(self._w, C.POINTER(C.c_uint32)), C.cast(self._h, C.POINTER(C.c_uint32)),
+                                C.cast(self._v, C.POINTER(C.c_uint32)) if self._v is not None else None)
         h = C.c_void_p()
         L.check(lib.irt_batch_create(ctx.handle, C.byref(self.desc), C.byref(h)), ctx.handle, "batch create")
         self.handle = h
@@ -51,6 +53,9 @@ class Batch:
     def autotune(self, frames: int):
         L.check(lib.irt_batch_autotune(self.handle, frames), self.ctx.handle, "batch autotune")
 
+    def set_waves(self, budget_px: int):
+        L.check(lib.irt_batch_set_waves(self.handle, budget_px), self.ctx.handle, "batch waves")
+
     def tuning(self) -> str:
         buf = C.create_string_buffer(256)
         L.check(lib.irt_batch_tuning(self.handle, buf, 256), self.ctx.handle, "batch tuning")
@@ -75,9 +80,13 @@ class BatchDriver:
 
     def __init__(self, ctx: Context, views, gbuffer_format=L.GBUFFER_F32, radiance_format=L.RADIANCE_F32,
                  moments_format=L.MOMENTS_F32, use_graphs=True):
-        """views: list of (Workload, camera phase offset) — each view follows
-        its workload's camera path shifted by the offset frames."""
+        """views: list of (Workload, camera phase offset[, (width, height)]) —
+        each view follows its workload's camera path shifted by the offset
+        frames, at the workload's frame size or the one given (views of a
+        scene share its projection, so any size of the same aspect works)."""
         self.ctx = ctx
+        self.sizes = [v[2] if len(v) > 2 else (v[0].width, v[0].height) for v in views]
+        views = [(v[0], v[1]) for v in views]
         self.views = views
         self.fmt = gbuffer_format
         wls = []
@@ -86,9 +95,9 @@ class BatchDriver:
                 wls.append(wl)
         self.wls = wls
         self.scenes = {id(wl): Scene(ctx, wl.meshes, wl.atlas, wl.sdf_format) for wl in wls}
-        self.batch = Batch(ctx, wls[0].settings, [(wl.width, wl.height) for wl, _ in views], gbuffer_format,
-                           radiance_format, moments_format, use_graphs)
-        self.gb = [gbuffer_device_alloc(wl.height, wl.width, gbuffer_format) for wl, _ in views]
+        self.batch = Batch(ctx, wls[0].settings, self.sizes, gbuffer_format, radiance_format, moments_format,
+                           use_graphs, [wl.settings.vpl_count for wl, _ in views])
+        self.gb = [gbuffer_device_alloc(h, w, gbuffer_format) for w, h in self.sizes]
         self.vpls = [[torch.zeros(wl.settings.vpl_count * 48, dtype=torch.uint8, device="cuda") for _ in range(2)]
                      for wl, _ in views]
         self.zero = [torch.zeros(wl.settings.vpl_count * 48, dtype=torch.uint8, device="cuda") for wl, _ in views]
@@ -104,6 +113,7 @@ class BatchDriver:
         sh = stream_handle()
         for v, ((wl, off), (f, obj, nodes, lights)) in enumerate(zip(self.views, data)):
             # every view's frame carries the batch's frame index and history flags
+            f.size[0], f.size[1] = self.sizes[v]
             f.size[2] = index
             f.flags[0] = 1 if index > 0 else 0
             f.flags[1] = f.size[3] if index > 0 else 0

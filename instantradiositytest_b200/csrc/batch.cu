@@ -12,7 +12,13 @@
 // as kernel parameters, so every view's results are identical to rendering
 // it alone.  Tables depend on the frame parity (SVGF ping-pong) and on the
 // caller's buffers; they are rebuilt (and graphs re-captured) when any
-// pointer or scene layout changes.  The batch works on a stream of its own
+// pointer or scene layout changes.
+// Views run in waves: consecutive views whose pixels add up to at most the
+// wave budget share one launch per pass, and the waves run one after
+// another, so a wave's buffers are still in L2 when its next pass reads them
+// (running every view pass by pass streams the whole batch through HBM
+// between passes).  The autotuner picks the wave budget (one wave = all
+// views) together with the tile shapes.  The batch works on a stream of its own
 // (a graph cannot be captured on the legacy default stream) that is joined
 // to the caller's stream with events in both directions.
 #include <cuda_runtime.h>
@@ -33,6 +39,9 @@ const Shape kShapes[] = {{32, 8}, {64, 4}, {16, 16}, {128, 2}, {256, 1}};
 constexpr int kNumShapes = 5;
 const int kMarchBps[] = {0, 5, 4};  // CTAs per SM for the march (0 = occupancy maximum)
 constexpr int kNumMarch = 3;
+// Wave budgets in pixels (0 = every view in one wave).
+const uint64_t kWavePx[] = {0, 8u << 20, 4u << 20, 2u << 20, 1u << 20};
+constexpr int kNumWaves = 5;
 
 // Tuned passes (2-D kernels).
 enum { kTReuse = 0, kTSpatial, kTTemporal, kTVariance, kTAtrous, kNumTuned };
@@ -49,9 +58,9 @@ struct ParityTables {
     void* largs = nullptr;         // LightArgs x n
     void* sviews[8] = {};          // SVGF records x n: temporal, variance, a-trous 0..3, guides, previous guides
     void* history = nullptr;       // history-copy records x n
-    MarchGroup* groups = nullptr;  // device
+    MarchGroup* groups = nullptr;  // device, grouped by wave
     MarchQueue* queues = nullptr;  // device
-    uint32_t n_groups = 0;
+    std::vector<uint32_t> wave_groups;  // groups of wave w: [wave_groups[w], wave_groups[w + 1])
     uint32_t max_scene_bytes = 0;
     cudaGraphExec_t graph = nullptr;
     int renders = 0;               // direct renders of this parity since the tables were built
@@ -63,7 +72,7 @@ struct irt_batch {
     irt_context* ctx = nullptr;
     irt_batch_desc desc{};
     uint32_t n = 0;
-    std::vector<uint32_t> W, H;
+    std::vector<uint32_t> W, H, vpls;
     std::vector<irt_session*> sess;
     int num_sms = 0;
     cudaStream_t stream = nullptr;
@@ -73,10 +82,14 @@ struct irt_batch {
     irt_frame* d_frames = nullptr;
     cudaEvent_t staged[2] = {nullptr, nullptr};  // the last use of h_frames[p] completed
     // tile tables: 2-D per candidate shape, 1-D (256 pixels)
+    // per wave w: n_w + 1 block offsets at entry wave_begin[w] + w
     uint32_t* d_tiles2[kNumShapes] = {};
-    uint32_t tiles2[kNumShapes] = {};
+    std::vector<uint32_t> tiles2[kNumShapes];
     uint32_t* d_tiles1 = nullptr;
-    uint32_t tiles1 = 0;
+    std::vector<uint32_t> tiles1;
+    std::vector<uint32_t> wave_begin;  // views of wave w: [wave_begin[w], wave_begin[w + 1])
+    uint64_t wave_budget = 0;         // pixels per wave (0 = all views in one wave)
+    size_t la = 0, sv = 0;             // bytes of a lighting / SVGF per-view record
     ParityTables par[2];
     // tuning
     int shape_of[kNumTuned] = {0, 0, 0, 0, 0};
@@ -84,6 +97,9 @@ struct irt_batch {
     uint32_t tune_left = 0, tune_total = 0;
     std::vector<double> tune_ms;  // [candidate][kNumTuned + 1]
     std::vector<int> tune_count;
+    double wave_ms[kNumWaves] = {};
+    int wave_count[kNumWaves] = {};
+    int tune_wave = -1;  // wave candidate being timed after the shapes (-1: none)
     cudaEvent_t ev[kNumEvents] = {};
     float pass_ms[kNumPass] = {};
     bool timed_pending = false;
@@ -114,6 +130,7 @@ void free_tables(ParityTables& t) {
     t.largs = t.history = nullptr;
     t.groups = nullptr;
     t.queues = nullptr;
+    t.wave_groups.clear();
     t.valid = false;
     t.renders = 0;
 }
@@ -189,8 +206,7 @@ irt_status build_tables(irt_batch* b, int p, irt_scene* const* scenes, const irt
     ParityTables& t = b->par[p];
     free_tables(t);
     const int cur_i = p, old_i = 1 - p;
-    const size_t la = irt_lighting_args_size(b->desc.gbuffer_format);
-    const size_t sv = irt_svgf_view_size(b->desc.gbuffer_format);
+    const size_t la = b->la, sv = b->sv;
     std::vector<unsigned char> hl(la * b->n);
     std::vector<std::vector<unsigned char>> hs(9, std::vector<unsigned char>(sv * b->n));
     const uint32_t iters = b->desc.settings.svgf_iterations;
@@ -250,41 +266,46 @@ irt_status build_tables(irt_batch* b, int p, irt_scene* const* scenes, const irt
     CK(upload(&t.largs, hl.data(), hl.size()), "batch lighting table");
     for (int k = 0; k < 8; k++) CK(upload(&t.sviews[k], hs[k].data(), hs[k].size()), "batch svgf table");
     CK(upload(&t.history, hs[8].data(), hs[8].size()), "batch history table");
-    // March: views grouped by scene, groups in order of first appearance.
-    std::vector<const irt_scene*> order;
-    for (uint32_t v = 0; v < b->n; v++)
-        if (std::find(order.begin(), order.end(), scenes[v]) == order.end()) order.push_back(scenes[v]);
+    // March: per wave, its views grouped by scene (groups in order of first
+    // appearance); a group's queues are its views' ray queues.
     std::vector<MarchGroup> groups;
     std::vector<MarchQueue> queues;
     t.max_scene_bytes = 0;
-    for (const irt_scene* sc : order) {
-        MarchGroup G{};
-        G.q_begin = (uint32_t)queues.size();
-        for (uint32_t v = 0; v < b->n; v++) {
-            if (scenes[v] != sc) continue;
-            if (queues.size() == G.q_begin) G.f = frames[v];
-            irt_session* s = b->sess[v];
-            queues.push_back(MarchQueue{s->rays, s->ray_counters, s->vis});
-            if (!G.error) G.error = s->error;
+    t.wave_groups.assign(1, 0);
+    for (size_t w = 0; w + 1 < b->wave_begin.size(); w++) {
+        const uint32_t v0 = b->wave_begin[w], v1 = b->wave_begin[w + 1];
+        std::vector<const irt_scene*> order;
+        for (uint32_t v = v0; v < v1; v++)
+            if (std::find(order.begin(), order.end(), scenes[v]) == order.end()) order.push_back(scenes[v]);
+        for (const irt_scene* sc : order) {
+            MarchGroup G{};
+            G.q_begin = (uint32_t)queues.size();
+            for (uint32_t v = v0; v < v1; v++) {
+                if (scenes[v] != sc) continue;
+                if (queues.size() == G.q_begin) G.f = frames[v];
+                irt_session* s = b->sess[v];
+                queues.push_back(MarchQueue{s->rays, s->ray_counters, s->vis});
+                if (!G.error) G.error = s->error;
+            }
+            G.q_end = (uint32_t)queues.size();
+            G.objects = sc->objects;
+            G.meshes = sc->meshes;
+            G.nodes = sc->nodes;
+            G.atlas = sc->atlas;
+            G.sdf_f16 = sc->sdf_f16;
+            G.march_scene = sc->march_scene;
+            const uint32_t bytes = irt_march_scene_bytes(sc->object_count);
+            G.scene_vec4 = bytes / 16;
+            t.max_scene_bytes = std::max(t.max_scene_bytes, bytes);
+            G.cells = sc->cells;
+            for (int a = 0; a < 3; a++) {
+                G.grid_org[a] = sc->grid_org[a];
+                G.grid_inv[a] = sc->grid_inv[a];
+            }
+            groups.push_back(G);
         }
-        G.q_end = (uint32_t)queues.size();
-        G.objects = sc->objects;
-        G.meshes = sc->meshes;
-        G.nodes = sc->nodes;
-        G.atlas = sc->atlas;
-        G.sdf_f16 = sc->sdf_f16;
-        G.march_scene = sc->march_scene;
-        const uint32_t bytes = irt_march_scene_bytes(sc->object_count);
-        G.scene_vec4 = bytes / 16;
-        t.max_scene_bytes = std::max(t.max_scene_bytes, bytes);
-        G.cells = sc->cells;
-        for (int a = 0; a < 3; a++) {
-            G.grid_org[a] = sc->grid_org[a];
-            G.grid_inv[a] = sc->grid_inv[a];
-        }
-        groups.push_back(G);
+        t.wave_groups.push_back((uint32_t)groups.size());
     }
-    t.n_groups = (uint32_t)groups.size();
     CK(upload(&t.groups, groups.data(), groups.size() * sizeof(MarchGroup)), "batch march groups");
     CK(upload(&t.queues, queues.data(), queues.size() * sizeof(MarchQueue)), "batch march queues");
     t.signature = signature_of(b, scenes, frames, g, cur, prev);
@@ -292,70 +313,127 @@ irt_status build_tables(irt_batch* b, int p, irt_scene* const* scenes, const irt
     return IRT_OK;
 }
 
-BatchLaunch batch_launch(const irt_batch* b, const void* table, int shape) {
+// Launch of one pass over wave w; `rec` is the byte size of a table record.
+BatchLaunch batch_launch(const irt_batch* b, size_t w, const void* table, size_t rec, int shape) {
+    const uint32_t v0 = b->wave_begin[w];
     BatchLaunch B{};
-    B.n = b->n;
-    B.frames = b->d_frames;
-    B.table = table;
+    B.n = b->wave_begin[w + 1] - v0;
+    B.frames = b->d_frames + v0;
+    B.table = static_cast<const char*>(table) + rec * v0;
     B.gbuffer_format = b->desc.gbuffer_format;
     B.radiance_f16 = b->desc.radiance_format == IRT_RADIANCE_F16;
     B.moments_f16 = b->desc.moments_format == IRT_MOMENTS_F16;
     if (shape >= 0) {
-        B.tile_start = b->d_tiles2[shape];
-        B.tiles = b->tiles2[shape];
+        B.tile_start = b->d_tiles2[shape] + v0 + w;
+        B.tiles = b->tiles2[shape][w];
         B.bx = kShapes[shape].bx;
         B.by = kShapes[shape].by;
     } else {
-        B.tile_start = b->d_tiles1;
-        B.tiles = b->tiles1;
+        B.tile_start = b->d_tiles1 + v0 + w;
+        B.tiles = b->tiles1[w];
         B.bx = 256;
         B.by = 1;
     }
     return B;
 }
 
-// The frame's launches on `st`; `timed` records the step events.
+// Waves for a pixel budget (0 = one wave) and their tile tables.
+irt_status set_waves(irt_batch* b, uint64_t budget) {
+    irt_context* ctx = b->ctx;
+    b->wave_begin.assign(1, 0);
+    uint64_t acc = 0;
+    for (uint32_t v = 0; v < b->n; v++) {
+        const uint64_t px = (uint64_t)b->W[v] * b->H[v];
+        if (budget && v > b->wave_begin.back() && acc + px > budget) {
+            b->wave_begin.push_back(v);
+            acc = 0;
+        }
+        acc += px;
+    }
+    b->wave_begin.push_back(b->n);
+    const size_t waves = b->wave_begin.size() - 1;
+    std::vector<uint32_t> start(b->n + waves);
+    auto build = [&](uint32_t bx, uint32_t by, std::vector<uint32_t>& tiles) {
+        tiles.assign(waves, 0);
+        for (size_t w = 0; w < waves; w++) {
+            uint32_t t = 0;
+            const uint32_t v0 = b->wave_begin[w], v1 = b->wave_begin[w + 1];
+            for (uint32_t v = v0; v < v1; v++) {
+                start[v + w] = t;
+                t += by ? ((b->W[v] + bx - 1) / bx) * ((b->H[v] + by - 1) / by)
+                        : (uint32_t)(((size_t)b->W[v] * b->H[v] + bx - 1) / bx);
+            }
+            start[v1 + w] = t;
+            tiles[w] = t;
+        }
+    };
+    for (int k = 0; k < kNumShapes; k++) {
+        build(kShapes[k].bx, kShapes[k].by, b->tiles2[k]);
+        if (b->d_tiles2[k]) cudaFree(b->d_tiles2[k]);  // the entry count follows the waves
+        b->d_tiles2[k] = nullptr;
+        CK(upload(&b->d_tiles2[k], start.data(), start.size() * 4), "batch tiles");
+    }
+    build(256, 0, b->tiles1);
+    if (b->d_tiles1) cudaFree(b->d_tiles1);
+    b->d_tiles1 = nullptr;
+    CK(upload(&b->d_tiles1, start.data(), start.size() * 4), "batch tiles");
+    b->wave_budget = budget;
+    for (auto& t : b->par) free_tables(t);  // march groups follow the waves
+    return IRT_OK;
+}
+
+// The frame's launches on `st`, wave after wave; `timed` records the events
+// (every step's when there is one wave, else the frame's start and end).
 irt_status launch_frame(irt_batch* b, int p, cudaStream_t st, const int shape_of[kNumTuned], int march_choice,
                         bool timed) {
     irt_context* ctx = b->ctx;
     ParityTables& t = b->par[p];
+    const size_t waves = b->wave_begin.size() - 1;
     auto mark = [&](int k) {
-        if (timed) cudaEventRecord(b->ev[k], st);
+        if (timed && (waves == 1 || k == 0 || k == kNumEvents - 1)) cudaEventRecord(b->ev[k], st);
     };
+    const size_t la = b->la, sv = b->sv;
     mark(0);
     CK(cudaMemcpyAsync(b->d_frames, b->h_frames[p], sizeof(irt_frame) * b->n, cudaMemcpyHostToDevice, st),
        "batch frames");
     mark(1);
-    CK(irt_launch_svgf_batched(batch_launch(b, t.sviews[6], -1), 3, st), "batch guides");
-    CK(irt_launch_svgf_batched(batch_launch(b, t.sviews[7], -1), 4, st), "batch previous guides");
-    mark(2);
-    CK(irt_launch_lighting_batched(batch_launch(b, t.largs, -1), kStageArchive, st), "batch archive");
-    mark(3);
-    CK(irt_launch_lighting_batched(batch_launch(b, t.largs, shape_of[kTReuse]), kStageReuse, st), "batch reuse");
-    mark(4);
-    CK(irt_launch_lighting_batched(batch_launch(b, t.largs, shape_of[kTSpatial]), kStageSpatial, st), "batch spatial");
-    mark(5);
-    MarchBatch M{};
-    M.n_groups = t.n_groups;
-    M.groups = t.groups;
-    M.queues = t.queues;
-    M.max_scene_bytes = t.max_scene_bytes;
-    M.num_sms = b->num_sms;
-    M.blocks_per_sm = kMarchBps[march_choice];
-    M.fast = 1;
-    CK(irt_launch_march_batched(M, st), "batch march");
-    mark(6);
-    CK(irt_launch_lighting_batched(batch_launch(b, t.largs, -1), kStageCombine, st), "batch combine");
-    mark(7);
-    CK(irt_launch_svgf_batched(batch_launch(b, t.sviews[0], shape_of[kTTemporal]), 0, st), "batch temporal");
-    mark(8);
-    CK(irt_launch_svgf_batched(batch_launch(b, t.sviews[1], shape_of[kTVariance]), 1, st), "batch variance");
-    mark(9);
-    const uint32_t iters = b->desc.settings.svgf_iterations;
-    for (uint32_t i = 0; i < iters && i < 4; i++)
-        CK(irt_launch_svgf_batched(batch_launch(b, t.sviews[2 + i], shape_of[kTAtrous]), 2, st), "batch atrous");
-    mark(10);
-    CK(irt_launch_svgf_batched(batch_launch(b, t.history, -1), 5, st), "batch history");
+    for (size_t w = 0; w < waves; w++) {
+        CK(irt_launch_svgf_batched(batch_launch(b, w, t.sviews[6], sv, -1), 3, st), "batch guides");
+        CK(irt_launch_svgf_batched(batch_launch(b, w, t.sviews[7], sv, -1), 4, st), "batch previous guides");
+        mark(2);
+        CK(irt_launch_lighting_batched(batch_launch(b, w, t.largs, la, -1), kStageArchive, st), "batch archive");
+        mark(3);
+        CK(irt_launch_lighting_batched(batch_launch(b, w, t.largs, la, shape_of[kTReuse]), kStageReuse, st),
+           "batch reuse");
+        mark(4);
+        CK(irt_launch_lighting_batched(batch_launch(b, w, t.largs, la, shape_of[kTSpatial]), kStageSpatial, st),
+           "batch spatial");
+        mark(5);
+        MarchBatch M{};
+        M.n_groups = t.wave_groups[w + 1] - t.wave_groups[w];
+        M.groups = t.groups + t.wave_groups[w];
+        M.queues = t.queues;
+        M.max_scene_bytes = t.max_scene_bytes;
+        M.num_sms = b->num_sms;
+        M.blocks_per_sm = kMarchBps[march_choice];
+        M.fast = 1;
+        CK(irt_launch_march_batched(M, st), "batch march");
+        mark(6);
+        CK(irt_launch_lighting_batched(batch_launch(b, w, t.largs, la, -1), kStageCombine, st), "batch combine");
+        mark(7);
+        CK(irt_launch_svgf_batched(batch_launch(b, w, t.sviews[0], sv, shape_of[kTTemporal]), 0, st),
+           "batch temporal");
+        mark(8);
+        CK(irt_launch_svgf_batched(batch_launch(b, w, t.sviews[1], sv, shape_of[kTVariance]), 1, st),
+           "batch variance");
+        mark(9);
+        const uint32_t iters = b->desc.settings.svgf_iterations;
+        for (uint32_t i = 0; i < iters && i < 4; i++)
+            CK(irt_launch_svgf_batched(batch_launch(b, w, t.sviews[2 + i], sv, shape_of[kTAtrous]), 2, st),
+               "batch atrous");
+        mark(10);
+        CK(irt_launch_svgf_batched(batch_launch(b, w, t.history, sv, -1), 5, st), "batch history");
+    }
     mark(11);
     return IRT_OK;
 }
@@ -386,6 +464,8 @@ irt_status irt_batch_create(irt_context* ctx, const irt_batch_desc* desc, irt_ba
     b->H.assign(desc->heights, desc->heights + b->n);
     b->desc.widths = b->W.data();
     b->desc.heights = b->H.data();
+    for (uint32_t v = 0; v < b->n; v++) b->vpls.push_back(desc->vpl_counts ? desc->vpl_counts[v] : desc->settings.vpl_count);
+    b->desc.vpl_counts = b->vpls.data();
     auto fail = [&](irt_status st) {
         irt_batch_destroy(b);
         return st;
@@ -395,6 +475,7 @@ irt_status irt_batch_create(irt_context* ctx, const irt_batch_desc* desc, irt_ba
         sd.settings = desc->settings;
         sd.settings.render_width = b->W[v];
         sd.settings.render_height = b->H[v];
+        sd.settings.vpl_count = b->vpls[v];
         sd.gbuffer_format = desc->gbuffer_format;
         sd.radiance_format = desc->radiance_format;
         sd.moments_format = desc->moments_format;
@@ -417,26 +498,12 @@ irt_status irt_batch_create(irt_context* ctx, const irt_batch_desc* desc, irt_ba
     if (cudaMalloc(&b->d_frames, sizeof(irt_frame) * b->n) != cudaSuccess) return fail(IRT_E_CUDA);
     for (auto& e : b->ev)
         if (cudaEventCreate(&e) != cudaSuccess) return fail(IRT_E_CUDA);
-    // Tile tables.
-    std::vector<uint32_t> start(b->n + 1);
-    for (int k = 0; k < kNumShapes; k++) {
-        uint32_t acc = 0;
-        for (uint32_t v = 0; v < b->n; v++) {
-            start[v] = acc;
-            acc += ((b->W[v] + kShapes[k].bx - 1) / kShapes[k].bx) * ((b->H[v] + kShapes[k].by - 1) / kShapes[k].by);
-        }
-        start[b->n] = acc;
-        b->tiles2[k] = acc;
-        if (upload(&b->d_tiles2[k], start.data(), start.size() * 4) != cudaSuccess) return fail(IRT_E_CUDA);
+    b->la = irt_lighting_args_size(desc->gbuffer_format);
+    b->sv = irt_svgf_view_size(desc->gbuffer_format);
+    {
+        irt_status st = set_waves(b, 0);  // one wave until tuned or set
+        if (st) return fail(st);
     }
-    uint32_t acc = 0;
-    for (uint32_t v = 0; v < b->n; v++) {
-        start[v] = acc;
-        acc += (uint32_t)(((size_t)b->W[v] * b->H[v] + 255) / 256);
-    }
-    start[b->n] = acc;
-    b->tiles1 = acc;
-    if (upload(&b->d_tiles1, start.data(), start.size() * 4) != cudaSuccess) return fail(IRT_E_CUDA);
     *out = b;
     return IRT_OK;
 }
@@ -474,7 +541,9 @@ irt_status irt_batch_autotune(irt_batch* b, uint32_t frames) {
     b->tune_total = b->tune_left = std::max<uint32_t>(frames, (uint32_t)C);
     b->tune_ms.assign((size_t)C * (kNumTuned + 1), 0.0);
     b->tune_count.assign(C, 0);
-    return IRT_OK;
+    b->tune_wave = -1;
+    for (int k = 0; k < kNumWaves; k++) b->wave_ms[k] = 0.0, b->wave_count[k] = 0;
+    return set_waves(b, 0);  // shapes are timed per pass on one wave
 }
 
 irt_status irt_batch_tuning(const irt_batch* b, char* out, size_t len) {
@@ -488,13 +557,32 @@ irt_status irt_batch_tuning(const irt_batch* b, char* out, size_t len) {
     }
     const int bps = kMarchBps[b->march_choice];
     s += "march_ctas_per_sm=" + (bps ? std::to_string(bps) : std::string("max"));
+    s += " waves=" + std::to_string(b->wave_begin.size() - 1) + " wave_budget_px=" +
+         (b->wave_budget ? std::to_string(b->wave_budget) : std::string("all"));
     std::snprintf(out, len, "%s", s.c_str());
     return IRT_OK;
+}
+
+irt_status irt_batch_set_waves(irt_batch* b, uint64_t budget_px) {
+    if (!b) return IRT_E_INVALID;
+    irt_context* ctx = b->ctx;
+    DeviceGuard dg(ctx->device);
+    CK(cudaStreamSynchronize(b->stream), "batch waves");
+    b->tune_wave = -1;
+    return set_waves(b, budget_px);
 }
 
 irt_status irt_batch_pass_ms(irt_batch* b, float* out12) {
     if (!b || !out12) return IRT_E_INVALID;
     irt_context* ctx = b->ctx;
+    if (b->timed_pending && b->wave_begin.size() > 2) {  // several waves: the frame's total only
+        CK(cudaEventSynchronize(b->ev[kNumEvents - 1]), "batch pass timing");
+        float total = 0.f;
+        cudaEventElapsedTime(&total, b->ev[0], b->ev[kNumEvents - 1]);
+        for (float& v : b->pass_ms) v = 0.f;
+        b->pass_ms[kPTotal] = total;
+        b->timed_pending = false;
+    }
     if (b->timed_pending) {
         CK(cudaEventSynchronize(b->ev[kNumEvents - 1]), "batch pass timing");
         float ms[kNumEvents - 1];
@@ -534,7 +622,7 @@ irt_status irt_batch_render(irt_batch* b, irt_scene* const* scenes, const irt_fr
             ctx->set_error("debug views are not batched");
             return IRT_E_INVALID;
         }
-        if (f.counts[1] != set.vpl_count || f.counts[3] != sc->object_count || f.counts[0] > sc->light_count ||
+        if (f.counts[1] != b->vpls[v] || f.counts[3] != sc->object_count || f.counts[0] > sc->light_count ||
             (uint32_t)f.rr[2] != set.restir_max_history) {
             ctx->set_error("batched frame counts differ from the batch/scene");
             return IRT_E_INVALID;
@@ -563,7 +651,10 @@ irt_status irt_batch_render(irt_batch* b, irt_scene* const* scenes, const irt_fr
     // Work on the batch stream follows everything queued on the caller's.
     CK(cudaEventRecord(b->join_in, caller), "batch join");
     CK(cudaStreamWaitEvent(st, b->join_in, 0), "batch join");
+    bool next_waves = false;
+    int waves_to = 0;
     if (b->tune_left > 0) {
+        // Phase 1: every candidate shape for all tuned passes (one wave).
         const int C = (int)b->tune_count.size();
         const int c = (int)((b->tune_total - b->tune_left) % (uint32_t)C);
         int shapes[kNumTuned];
@@ -601,11 +692,28 @@ irt_status irt_batch_render(irt_batch* b, irt_scene* const* scenes, const irt_fr
             for (int k = 1; k < kNumMarch; k++)
                 if (cnt[k] && (!cnt[best] || sum[k] / cnt[k] < sum[best] / cnt[best])) best = k;
             b->march_choice = best;
-            for (auto& tb : b->par) {  // shapes changed: graphs are captured again
-                if (tb.graph) cudaGraphExecDestroy(tb.graph);
-                tb.graph = nullptr;
-                tb.renders = 0;
-            }
+            b->tune_wave = 0;  // phase 2 starts with one wave (the tables in use)
+        }
+        b->pass_ms[kPGraph] = 0.f;
+    } else if (b->tune_wave >= 0) {
+        // Phase 2: each wave budget with the chosen shapes, timed per frame.
+        irt_status rc = launch_frame(b, p, st, b->shape_of, b->march_choice, true);
+        if (rc) return rc;
+        CK(cudaEventSynchronize(b->ev[kNumEvents - 1]), "batch tuning");
+        float ms = 0.f;
+        cudaEventElapsedTime(&ms, b->ev[0], b->ev[kNumEvents - 1]);
+        b->wave_ms[b->tune_wave] += ms;
+        b->wave_count[b->tune_wave]++;
+        next_waves = true;
+        if (b->tune_wave + 1 < kNumWaves) {
+            waves_to = ++b->tune_wave;
+        } else {
+            int best = 0;
+            for (int k = 1; k < kNumWaves; k++)
+                if (b->wave_count[k] && b->wave_ms[k] / b->wave_count[k] < b->wave_ms[best] / b->wave_count[best])
+                    best = k;
+            waves_to = best;
+            b->tune_wave = -1;
         }
         b->pass_ms[kPGraph] = 0.f;
     } else if (b->desc.use_graphs && t.graph) {
@@ -634,6 +742,11 @@ irt_status irt_batch_render(irt_batch* b, irt_scene* const* scenes, const irt_fr
         t.renders++;
         b->timed_pending = true;  // read (with a sync) only when asked for
         b->pass_ms[kPGraph] = 0.f;
+    }
+    if (next_waves) {  // the next frame runs the next wave budget (tables rebuilt then)
+        CK(cudaStreamSynchronize(st), "batch tuning");
+        irt_status rc = set_waves(b, kWavePx[waves_to]);
+        if (rc) return rc;
     }
     CK(cudaEventRecord(b->staged[p], st), "batch staging event");
     CK(cudaEventRecord(b->join_out, st), "batch join");

@@ -152,6 +152,16 @@ __device__ __forceinline__ uint32_t svgf_find_view(const uint32_t* __restrict__ 
     }
     return lo;
 }
+// Copies a view's record into shared memory (4-byte words, every thread of
+// the block), so the per-pixel code reads it like kernel parameters.
+template <class T>
+__device__ __forceinline__ void svgf_stage(const T* __restrict__ src, T* dst) {
+    static_assert(sizeof(T) % 4 == 0, "records are whole words");
+    const uint32_t* s = reinterpret_cast<const uint32_t*>(src);
+    uint32_t* d = reinterpret_cast<uint32_t*>(dst);
+    const uint32_t tid = threadIdx.y * blockDim.x + threadIdx.x, nt = blockDim.x * blockDim.y;
+    for (uint32_t i = tid; i < sizeof(T) / 4; i += nt) d[i] = __ldg(s + i);
+}
 // Pixel of this thread in 2-D tile t of a view of width W.
 __device__ __forceinline__ void svgf_tile_xy(uint32_t W, uint32_t t, int32_t& x, int32_t& y) {
     uint32_t tiles_x = (W + blockDim.x - 1) / blockDim.x;

@@ -473,14 +473,30 @@ __device__ __forceinline__ void tile_xy(const irt_frame& f, uint32_t t, uint32_t
     y = (t / tiles_x) * blockDim.y + threadIdx.y;
 }
 
+// Copies a view's record into shared memory (4-byte words, every thread of
+// the block), so the per-pixel code reads it like kernel parameters: from
+// on-chip memory that no global store can alias.
+template <class T>
+__device__ __forceinline__ void stage_record(const T* __restrict__ src, T* dst) {
+    static_assert(sizeof(T) % 4 == 0, "records are whole words");
+    const uint32_t* s = reinterpret_cast<const uint32_t*>(src);
+    uint32_t* d = reinterpret_cast<uint32_t*>(dst);
+    const uint32_t tid = threadIdx.y * blockDim.x + threadIdx.x, nt = blockDim.x * blockDim.y;
+    for (uint32_t i = tid; i < sizeof(T) / 4; i += nt) d[i] = __ldg(s + i);
+}
+
 template <class G>
 __global__ void __launch_bounds__(256) reuse_batched(const irt_frame* __restrict__ frames, const LightArgs<G>* __restrict__ args,
                                                      const uint32_t* __restrict__ tile_start, uint32_t n, int keep) {
     const uint32_t v = find_view(tile_start, n, blockIdx.x);
-    const irt_frame& f = frames[v];
+    __shared__ __align__(16) irt_frame f;
+    __shared__ __align__(16) LightArgs<G> a;
+    stage_record(frames + v, &f);
+    stage_record(args + v, &a);
+    __syncthreads();
     uint32_t x, y;
     tile_xy(f, blockIdx.x - __ldg(tile_start + v), x, y);
-    reuse_body<G>(f, args[v], keep, x, y);
+    reuse_body<G>(f, a, keep, x, y);
 }
 
 template <class G, class R>
@@ -488,10 +504,14 @@ __global__ void __launch_bounds__(256) spatial_prep_batched(const irt_frame* __r
                                                             const LightArgs<G>* __restrict__ args,
                                                             const uint32_t* __restrict__ tile_start, uint32_t n) {
     const uint32_t v = find_view(tile_start, n, blockIdx.x);
-    const irt_frame& f = frames[v];
+    __shared__ __align__(16) irt_frame f;
+    __shared__ __align__(16) LightArgs<G> a;
+    stage_record(frames + v, &f);
+    stage_record(args + v, &a);
+    __syncthreads();
     uint32_t x, y;
     tile_xy(f, blockIdx.x - __ldg(tile_start + v), x, y);
-    spatial_prep_body<G, R>(f, args[v], x, y);
+    spatial_prep_body<G, R>(f, a, x, y);
 }
 
 template <class G, class R>

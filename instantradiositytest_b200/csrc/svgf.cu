@@ -131,8 +131,11 @@ __global__ void __launch_bounds__(256) svgf_temporal_batched(const irt_frame* __
                                                              const SView<G>* __restrict__ views,
                                                              const uint32_t* __restrict__ tile_start, uint32_t n) {
     const uint32_t v = svgf_find_view(tile_start, n, blockIdx.x);
-    const irt_frame& f = frames[v];
-    const SView<G>& w = views[v];
+    __shared__ __align__(16) irt_frame f;
+    __shared__ __align__(16) SView<G> w;
+    svgf_stage(frames + v, &f);
+    svgf_stage(views + v, &w);
+    __syncthreads();
     int32_t x, y;
     svgf_tile_xy(f.size[0], blockIdx.x - __ldg(tile_start + v), x, y);
     typedef typename R::T T;

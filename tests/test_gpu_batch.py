@@ -58,15 +58,15 @@ def test_batch_views_equal_alone(cuda, formats):
     views = [(a, 0), (b, 0), (a, 7), (c, 2), (b, 11)]
     ctx = Context()
     drv = BatchDriver(ctx, views, fmt, rfmt, mfmt, use_graphs=True)
-    drv.batch.autotune(5)
-    n_frames = 12
+    drv.batch.autotune(5)  # 5 shape frames, then 5 wave-budget frames
+    n_frames = 16
     per_view = [[] for _ in views]
     for i in range(n_frames):
         data = drv.inputs(i)
         frames = drv.step(i, data)
         for v, (f, (_, obj, nodes, lights)) in enumerate(zip(frames, data)):
             per_view[v].append((L.Frame.from_buffer_copy(f), obj, nodes, lights))
-        if i == 6:
+        if i == 11:
             print("passes", drv.batch.pass_ms())
     torch.cuda.synchronize()
     print("tuning:", drv.batch.tuning())
@@ -80,5 +80,31 @@ def test_batch_views_equal_alone(cuda, formats):
         for d in (0, 1):
             assert np.array_equal(s.reservoirs_host(d, 2).view(np.uint8), ref["res"][d]), (v, d)
         assert np.abs(got[L.BUF_DIRECT].view(np.float32)).max() > 0
+    drv.close()
+    ctx.close()
+
+
+def test_batch_in_waves_equals_alone(cuda):
+    """Views split into waves (several launches per pass, one per wave)."""
+    a = workload(31, 10, 160, 100)
+    b = workload(32, 14, 128, 80)
+    views = [(a, 0), (b, 0), (a, 5), (b, 9), (a, 13)]
+    ctx = Context()
+    drv = BatchDriver(ctx, views, use_graphs=True)
+    drv.batch.set_waves(30000)  # 160x100 + 128x80 views: waves of one or two views
+    per_view = [[] for _ in views]
+    for i in range(6):
+        data = drv.inputs(i)
+        frames = drv.step(i, data)
+        for v, (f, (_, obj, nodes, lights)) in enumerate(zip(frames, data)):
+            per_view[v].append((L.Frame.from_buffer_copy(f), obj, nodes, lights))
+    torch.cuda.synchronize()
+    print("tuning:", drv.batch.tuning())
+    assert "waves=1 " not in drv.batch.tuning()
+    for v, (wl, _) in enumerate(views):
+        s = drv.batch.view(v)
+        ref = render_alone(ctx, wl, per_view[v], L.GBUFFER_F32, L.RADIANCE_F32, L.MOMENTS_F32)
+        for w in BUFS:
+            assert np.array_equal(s.buffer(w, torch.uint8).cpu().numpy(), ref[w]), (v, w)
     drv.close()
     ctx.close()
