@@ -392,6 +392,15 @@ irt_status irt_gbuffer_render(irt_context* ctx, const irt_workload* wl, const ir
 irt_status irt_vpl_generate(irt_scene* scene, const irt_workload* wl, const irt_frame* frame,
                             irt_vpl* out, void* stream);
 
+/* Presentation pass (present.wgsl:1-8 drawn into the Rgba8UnormSrgb display
+ * target, src/renderer.rs:1300-1306, :1961): each pixel of a radiance image
+ * (IRT_RADIANCE_* format, e.g. IRT_BUF_FILTERED), clamped to [0, 1],
+ * sRGB-encoded and rounded to 8 bits, alpha 255; rgba8 is a device buffer of
+ * width*height*4 bytes.  Capture to PNG (src/renderer.rs:2109-2163) is the
+ * host's: read rgba8 back and encode it (instantradiositytest_b200.present). */
+irt_status irt_present(const void* radiance, int32_t radiance_format, uint32_t width, uint32_t height,
+                       uint8_t* rgba8, void* stream);
+
 /* ---------------------------------------------------------------------------
  * Batched views (no counterpart in the reference, which renders one view per
  * Renderer).  A batch renders many views of uneven size — each a session of

@@ -203,6 +203,7 @@ _PROTOS = {
     "irt_workload_vpls_cpu": (I32, [P, C.POINTER(Frame), P, P, P]),
     "irt_gbuffer_render": (I32, [P, P, C.POINTER(Frame), P, I32, P, P, P, P, P, P]),
     "irt_vpl_generate": (I32, [P, P, C.POINTER(Frame), P, P]),
+    "irt_present": (I32, [P, I32, U32, U32, P, P]),
     "irt_batch_create": (I32, [P, C.POINTER(BatchDesc), C.POINTER(P)]),
     "irt_batch_render": (I32, [P, P, C.POINTER(Frame), C.POINTER(GBuffer), P, P, P]),
     "irt_batch_view": (P, [P, U32]),
