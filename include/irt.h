@@ -248,6 +248,25 @@ irt_status irt_render_frame(irt_session* s, const irt_scene* scene, const irt_fr
                             const irt_gbuffer* gbuffer, const irt_vpl* current_vpls,
                             const irt_vpl* previous_vpls, void* stream);
 
+/* irt_render_frame from HOST inputs, pipelined: the G-buffer planes
+ * (host_gbuffer holds host pointers, pinned for the copies to overlap) and
+ * the VPL pool are copied into library-owned device staging (two G-buffer
+ * slots, three VPL pools, created on the first call) on the session's own
+ * copy stream while the previous frame still renders on `stream`; the frame
+ * renders on `stream` once its inputs have landed, and, with out_host, its
+ * filtered image (radiance format) is copied back to out_host on the copy
+ * stream.  Call irt_session_host_sync before reading out_host.  The
+ * previous VPL pool of a call is the pool of the session's previous call
+ * (zeros on the first).  No counterpart in the reference (its inputs are
+ * GPU render targets). */
+irt_status irt_render_frame_host(irt_session* s, const irt_scene* scene, const irt_frame* frame,
+                                 const irt_gbuffer* host_gbuffer, const irt_vpl* host_vpls, void* out_host,
+                                 void* stream);
+/* The host copies (inputs consumed, outputs written) of every
+ * irt_render_frame_host call so far: with stream == NULL the host waits for
+ * them; otherwise work queued on `stream` afterwards waits for them. */
+irt_status irt_session_host_sync(irt_session* s, void* stream);
+
 #define IRT_BUF_DIRECT 0          /* f32x4: resolve_direct output            */
 #define IRT_BUF_NOISY 1           /* radiance fmt: resolve_indirect output   */
 #define IRT_BUF_FILTERED 2        /* radiance fmt: SVGF output of the frame  */

@@ -172,6 +172,8 @@ _PROTOS = {
     "irt_frame_lighting": (I32, [P, P, C.POINTER(Frame), C.POINTER(GBuffer), P, P, P]),
     "irt_frame_svgf": (I32, [P, C.POINTER(Frame), C.POINTER(GBuffer), P]),
     "irt_render_frame": (I32, [P, P, C.POINTER(Frame), C.POINTER(GBuffer), P, P, P]),
+    "irt_render_frame_host": (I32, [P, P, C.POINTER(Frame), C.POINTER(GBuffer), P, P, P]),
+    "irt_session_host_sync": (I32, [P, P]),
     "irt_session_buffer": (I32, [P, I32, C.POINTER(P), C.POINTER(U64)]),
     "irt_session_reservoirs": (I32, [P, I32, I32, C.POINTER(P), C.POINTER(U64)]),
     "irt_session_check": (I32, [P, P]),

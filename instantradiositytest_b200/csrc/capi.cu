@@ -175,10 +175,32 @@ irt_status irt_scene_update(irt_scene* sc, const irt_object* objects, uint32_t o
         sc->bytes += added;
         ctx->in_use += added;
     }
-    CK(cudaMemcpyAsync(sc->objects, objects, sizeof(irt_object) * object_count, cudaMemcpyHostToDevice, st), "objects");
-    CK(cudaMemcpyAsync(sc->nodes, nodes, sizeof(irt_node) * node_count, cudaMemcpyHostToDevice, st), "nodes");
+    // Per-frame data goes through a pinned staging slot: the copies are then
+    // truly asynchronous (a copy from pageable memory can hold the host until
+    // the stream drains), and the slot is reused only after its copies ran.
+    const size_t ob = sizeof(irt_object) * object_count, nb = sizeof(irt_node) * node_count,
+                 lb = sizeof(irt_light) * light_count;
+    const uint32_t mbytes_up = irt_march_scene_bytes(object_count);
+    const size_t need = ob + nb + lb + mbytes_up + 64;
+    const int slot = (int)(sc->updates % 2u);
+    if (!sc->pinned_free[slot]) CK(cudaEventCreateWithFlags(&sc->pinned_free[slot], cudaEventDisableTiming), "staging");
+    CK(cudaEventSynchronize(sc->pinned_free[slot]), "staging");
+    if (sc->pinned_cap[slot] < need) {
+        if (sc->pinned[slot]) cudaFreeHost(sc->pinned[slot]);
+        sc->pinned[slot] = nullptr;
+        sc->pinned_cap[slot] = 0;
+        CK(cudaMallocHost(&sc->pinned[slot], need), "staging");
+        sc->pinned_cap[slot] = need;
+    }
+    unsigned char* stage = sc->pinned[slot];
+    std::memcpy(stage, objects, ob);
+    std::memcpy(stage + ob, nodes, nb);
+    if (lb) std::memcpy(stage + ob + nb, lights, lb);
+    unsigned char* stage_march = stage + ((ob + nb + lb + 15) & ~size_t(15));
+    CK(cudaMemcpyAsync(sc->objects, stage, ob, cudaMemcpyHostToDevice, st), "objects");
+    CK(cudaMemcpyAsync(sc->nodes, stage + ob, nb, cudaMemcpyHostToDevice, st), "nodes");
     if (light_count) {
-        CK(cudaMemcpyAsync(sc->lights, lights, sizeof(irt_light) * light_count, cudaMemcpyHostToDevice, st), "lights");
+        CK(cudaMemcpyAsync(sc->lights, stage + ob + nb, lb, cudaMemcpyHostToDevice, st), "lights");
         CK(irt_launch_prepare_lights(sc->lights, light_count, sc->lights_prep, st), "light preparation");
     }
     // Compact march scene: the same values, laid out for shared memory.
@@ -224,7 +246,10 @@ irt_status irt_scene_update(irt_scene* sc, const irt_object* objects, uint32_t o
         mo[i].sphere = make_float4(m.enclosing_sphere[0], m.enclosing_sphere[1], m.enclosing_sphere[2],
                                    m.enclosing_sphere[3]);
     }
-    CK(cudaMemcpyAsync(sc->march_scene, sc->march_host.data(), mbytes, cudaMemcpyHostToDevice, st), "march scene");
+    std::memcpy(stage_march, sc->march_host.data(), mbytes);
+    CK(cudaMemcpyAsync(sc->march_scene, stage_march, mbytes, cudaMemcpyHostToDevice, st), "march scene");
+    CK(cudaEventRecord(sc->pinned_free[slot], st), "staging");
+    sc->updates++;
     // Leaf-order cache, rebuilt on the device when the BVH or an object
     // changes (static scenes build it once).
     if (sc->cached_nodes.size() != node_count || sc->cached_objects.size() != object_count ||
@@ -310,6 +335,13 @@ void irt_scene_destroy(irt_scene* sc) {
     if (sc->march_scene) cudaFree(sc->march_scene);
     if (sc->cells) cudaFree(sc->cells);
     if (sc->corners) cudaFree(sc->corners);
+    for (int k = 0; k < 2; k++) {
+        if (sc->pinned_free[k]) {
+            cudaEventSynchronize(sc->pinned_free[k]);
+            cudaEventDestroy(sc->pinned_free[k]);
+        }
+        if (sc->pinned[k]) cudaFreeHost(sc->pinned[k]);
+    }
     if (sc->ctx->in_use >= sc->bytes) sc->ctx->in_use -= sc->bytes;
     delete sc;
 }
@@ -423,6 +455,20 @@ void irt_session_destroy(irt_session* s) {
                     s->rays, s->ray_counters, s->vis, s->pending, s->guide[0], s->guide[1]};
     for (void* p : ptrs)
         if (p) cudaFree(p);
+    if (s->pipe.ready) {
+        irt_session::HostPipe& hp = s->pipe;
+        if (hp.copy) cudaStreamSynchronize(hp.copy);
+        if (hp.copy_out) cudaStreamSynchronize(hp.copy_out);
+        for (void* p : {hp.gbuf[0], hp.gbuf[1], (void*)hp.vpls, hp.out[0], hp.out[1]})
+            if (p) cudaFree(p);
+        for (cudaEvent_t e : {hp.copied[0], hp.copied[1], hp.rendered[0], hp.rendered[1], hp.vpl_free[0],
+                              hp.vpl_free[1], hp.vpl_free[2], hp.out_ready[0], hp.out_ready[1], hp.out_done[0],
+                              hp.out_done[1], hp.march_done})
+            if (e) cudaEventDestroy(e);
+        if (hp.copy) cudaStreamDestroy(hp.copy);
+        if (hp.copy_out) cudaStreamDestroy(hp.copy_out);
+        if (s->ctx->in_use >= hp.bytes) s->ctx->in_use -= hp.bytes;
+    }
     if (s->ev_ready)
         for (auto& row : s->ev)
             for (cudaEvent_t e : row) cudaEventDestroy(e);
@@ -559,6 +605,7 @@ irt_status irt_frame_lighting(irt_session* s, const irt_scene* sc, const irt_fra
         M.num_sms = s->num_sms;
         M.fast = s->desc.exact_march ? 0 : 1;
         CK(irt_launch_march(M, st), "march kernel");
+        if (s->pipe.ready) CK(cudaEventRecord(s->pipe.march_done, st), "pipeline event");
         mark(s, 4, st);
         CK(irt_launch_lighting(L, kStageCombine, st), "combine kernel");
         mark(s, 5, st);
@@ -656,6 +703,137 @@ irt_status irt_render_frame(irt_session* s, const irt_scene* sc, const irt_frame
     irt_status r = irt_frame_lighting(s, sc, f, g, cur, prev, stream);
     if (r) return r;
     return irt_frame_svgf(s, f, g, stream);
+}
+
+// ------------------------------------------------------------------ host inputs
+static uint64_t plane_bytes(int fmt, int k, size_t P) {
+    static const uint64_t b[3][5] = {{4, 16, 16, 8, 8}, {4, 8, 8, 4, 4}, {4, 4, 4, 4, 4}};
+    return b[fmt][k] * P;
+}
+
+static irt_status pipe_setup(irt_session* s) {
+    irt_context* ctx = s->ctx;
+    irt_session::HostPipe& hp = s->pipe;
+    const size_t P = s->P;
+    const int fmt = s->desc.gbuffer_format;
+    uint64_t gb = 0;
+    for (int k = 0; k < 5; k++) gb += plane_bytes(fmt, k, P);
+    const uint64_t pool = (uint64_t)s->desc.settings.vpl_count * sizeof(irt_vpl);
+    const uint64_t need = 2 * gb + 4 * pool + 2 * P * s->rad_bytes;
+    uint64_t cur = ctx->in_use.load();
+    for (;;) {
+        if (cur + need > ctx->budget) {
+            ctx->set_error("host-input staging exceeds the HBM budget");
+            return IRT_E_ADMISSION;
+        }
+        if (ctx->in_use.compare_exchange_weak(cur, cur + need)) break;
+    }
+    hp.bytes = need;
+    hp.ready = true;  // from here irt_session_destroy releases what exists
+    uint64_t used = 0;
+    CK(cudaStreamCreateWithFlags(&hp.copy, cudaStreamNonBlocking), "copy stream");
+    CK(cudaStreamCreateWithFlags(&hp.copy_out, cudaStreamNonBlocking), "copy stream");
+    for (int k = 0; k < 2; k++) {
+        irt_status st = dev_alloc(ctx, &hp.gbuf[k], gb, used);
+        if (!st) st = dev_alloc(ctx, &hp.out[k], P * s->rad_bytes, used);
+        if (st) return st;
+    }
+    irt_status st = dev_alloc(ctx, &hp.vpls, 4 * pool, used);  // zero-filled: pool [3] stays zero
+    if (st) return st;
+    for (cudaEvent_t* e : {&hp.copied[0], &hp.copied[1], &hp.rendered[0], &hp.rendered[1], &hp.vpl_free[0],
+                           &hp.vpl_free[1], &hp.vpl_free[2], &hp.out_ready[0], &hp.out_ready[1], &hp.out_done[0],
+                           &hp.out_done[1], &hp.march_done})
+        CK(cudaEventCreateWithFlags(e, cudaEventDisableTiming), "pipeline events");
+    return IRT_OK;
+}
+
+irt_status irt_render_frame_host(irt_session* s, const irt_scene* sc, const irt_frame* f, const irt_gbuffer* host_g,
+                                 const irt_vpl* host_vpls, void* out_host, void* stream) {
+    if (!s || !sc || !f || !host_g || !host_vpls) return IRT_E_INVALID;
+    irt_context* ctx = s->ctx;
+    if (host_g->format != s->desc.gbuffer_format || !host_g->depth || !host_g->normal || !host_g->color ||
+        !host_g->params || !host_g->motion) {
+        ctx->set_error("G-buffer format or planes invalid");
+        return IRT_E_INVALID;
+    }
+    DeviceGuard dg(ctx->device);
+    irt_session::HostPipe& hp = s->pipe;
+    if (!hp.ready) {
+        irt_status st = pipe_setup(s);
+        if (st) return st;
+    }
+    cudaStream_t st = static_cast<cudaStream_t>(stream);
+    const size_t P = s->P;
+    const int fmt = s->desc.gbuffer_format;
+    const int slot = (int)(hp.calls % 2u);
+    const int vslot = (hp.last_vpl + 1) % 3;
+    // Inputs, on the copy stream: the G-buffer slot and the VPL pool may be
+    // overwritten once the frames that read them have rendered.
+    CK(cudaStreamWaitEvent(hp.copy, hp.rendered[slot], 0), "pipeline wait");
+    CK(cudaStreamWaitEvent(hp.copy, hp.vpl_free[vslot], 0), "pipeline wait");
+    // Uploads run after the previous frame's march, beside its SVGF passes:
+    // the copies stream through L2, and during the march (which lives on
+    // L2-resident scene records, leaf cache and SDF texels) they slowed the
+    // frame by more than the copy takes.
+    CK(cudaStreamWaitEvent(hp.copy, hp.march_done, 0), "pipeline wait");
+    const void* src[5] = {host_g->depth, host_g->normal, host_g->color, host_g->params, host_g->motion};
+    char* base = static_cast<char*>(hp.gbuf[slot]);
+    const void* dst[5];
+    uint64_t off = 0;
+    for (int k = 0; k < 5; k++) {
+        dst[k] = base + off;
+        CK(cudaMemcpyAsync(base + off, src[k], plane_bytes(fmt, k, P), cudaMemcpyHostToDevice, hp.copy), "G-buffer in");
+        off += plane_bytes(fmt, k, P);
+    }
+    const uint64_t pool = (uint64_t)s->desc.settings.vpl_count * sizeof(irt_vpl);
+    irt_vpl* cur = hp.vpls + (size_t)vslot * s->desc.settings.vpl_count;
+    const irt_vpl* prev = hp.last_vpl < 0 ? hp.vpls + 3ull * s->desc.settings.vpl_count
+                                          : hp.vpls + (size_t)hp.last_vpl * s->desc.settings.vpl_count;
+    CK(cudaMemcpyAsync(cur, host_vpls, pool, cudaMemcpyHostToDevice, hp.copy), "VPLs in");
+    CK(cudaEventRecord(hp.copied[slot], hp.copy), "pipeline event");
+    // The frame, on the caller's stream, once its inputs have landed.
+    CK(cudaStreamWaitEvent(st, hp.copied[slot], 0), "pipeline wait");
+    irt_gbuffer g{fmt, static_cast<const float*>(dst[0]), dst[1], dst[2], dst[3], dst[4]};
+    irt_status r = irt_render_frame(s, sc, f, &g, cur, prev, stream);
+    if (r) return r;
+    CK(cudaEventRecord(hp.rendered[slot], st), "pipeline event");
+    // The pool this frame read as `previous` is free after it; the current
+    // one is the next frame's previous.
+    if (hp.last_vpl >= 0) CK(cudaEventRecord(hp.vpl_free[hp.last_vpl], st), "pipeline event");
+    if (out_host) {
+        // A device copy of the output (the next frame overwrites the image),
+        // then the host copy on the copy stream.
+        CK(cudaStreamWaitEvent(st, hp.out_done[slot], 0), "pipeline wait");
+        CK(cudaMemcpyAsync(hp.out[slot], s->filtered, P * s->rad_bytes, cudaMemcpyDeviceToDevice, st), "output");
+        CK(cudaEventRecord(hp.out_ready[slot], st), "pipeline event");
+        CK(cudaStreamWaitEvent(hp.copy_out, hp.out_ready[slot], 0), "pipeline wait");
+        CK(cudaMemcpyAsync(out_host, hp.out[slot], P * s->rad_bytes, cudaMemcpyDeviceToHost, hp.copy_out), "output");
+        CK(cudaEventRecord(hp.out_done[slot], hp.copy_out), "pipeline event");
+    }
+    hp.last_vpl = vslot;
+    hp.calls++;
+    return IRT_OK;
+}
+
+irt_status irt_session_host_sync(irt_session* s, void* stream) {
+    if (!s) return IRT_E_INVALID;
+    irt_context* ctx = s->ctx;
+    if (!s->pipe.ready) return IRT_OK;
+    DeviceGuard dg(ctx->device);
+    if (!stream) {
+        CK(cudaStreamSynchronize(s->pipe.copy), "host inputs");
+        CK(cudaStreamSynchronize(s->pipe.copy_out), "host outputs");
+        return IRT_OK;
+    }
+    for (cudaStream_t c : {s->pipe.copy, s->pipe.copy_out}) {
+        cudaEvent_t e;
+        CK(cudaEventCreateWithFlags(&e, cudaEventDisableTiming), "host join");
+        cudaError_t r = cudaEventRecord(e, c);
+        if (r == cudaSuccess) r = cudaStreamWaitEvent(static_cast<cudaStream_t>(stream), e, 0);
+        cudaEventDestroy(e);
+        CK(r, "host join");
+    }
+    return IRT_OK;
 }
 
 irt_status irt_session_buffer(irt_session* s, int32_t which, void** ptr, uint64_t* bytes) {

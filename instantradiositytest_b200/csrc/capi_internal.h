@@ -44,6 +44,12 @@ struct irt_scene {
     // compact march scene (nodes + object records with their mesh folded in)
     float4* march_scene = nullptr;
     std::vector<float4> march_host;
+    // Pinned staging of the per-frame uploads, two slots used in turn, so an
+    // update neither waits for the device nor races an earlier copy.
+    unsigned char* pinned[2] = {nullptr, nullptr};
+    size_t pinned_cap[2] = {0, 0};
+    cudaEvent_t pinned_free[2] = {nullptr, nullptr};
+    uint32_t updates = 0;
     // leaf-order cache (rebuilt when the BVH changes)
     uint4* cells = nullptr;
     float* corners = nullptr;
@@ -93,6 +99,23 @@ struct irt_session {
     float4* guide[2] = {nullptr, nullptr};
     uint32_t guide_frame = 0xffffffffu;
     int num_sms = 0;
+    // Host-input pipeline (irt_render_frame_host), created on first use:
+    // a copy stream, double-buffered device G-buffers, three VPL pools plus
+    // a zero pool, double-buffered device copies of the output image.
+    struct HostPipe {
+        bool ready = false;
+        cudaStream_t copy = nullptr;      // host -> device inputs
+        cudaStream_t copy_out = nullptr;  // device -> host outputs (own stream: an output copy
+                                          // waits for its frame, the next inputs must not)
+        void* gbuf[2] = {nullptr, nullptr};
+        irt_vpl* vpls = nullptr;      // 4 pools: [0..2] ring, [3] zeros
+        void* out[2] = {nullptr, nullptr};
+        cudaEvent_t copied[2] = {}, rendered[2] = {}, vpl_free[3] = {}, out_ready[2] = {}, out_done[2] = {};
+        cudaEvent_t march_done = nullptr;  // after the last frame's march (recorded by irt_frame_lighting)
+        uint32_t calls = 0;
+        int last_vpl = -1;
+        uint64_t bytes = 0;
+    } pipe;
     bool ev_ready = false;
     int prof_slot = 0;
     uint32_t prof_frame[kProfRing] = {};

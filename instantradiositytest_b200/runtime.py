@@ -112,6 +112,20 @@ class Session:
         L.check(lib.irt_render_frame(self.handle, scene.handle, C.byref(frame), C.byref(gbuffer), cur, prev,
                                      stream if stream is not None else stream_handle()), self.ctx.handle, "frame")
 
+    def render_host(self, scene, frame, host_gbuffer: L.GBuffer, host_vpls, out_host=None, stream=None):
+        """irt_render_frame_host: host (pinned) G-buffer planes and VPL pool in,
+        the filtered image to out_host (a pinned uint8 tensor) out; pipelined
+        with the previous call.  host_vpls / out_host: torch CPU tensors."""
+        L.check(lib.irt_render_frame_host(self.handle, scene.handle, C.byref(frame), C.byref(host_gbuffer),
+                                          C.c_void_p(host_vpls.data_ptr()),
+                                          C.c_void_p(out_host.data_ptr()) if out_host is not None else None,
+                                          stream if stream is not None else stream_handle()),
+                self.ctx.handle, "render host")
+
+    def host_sync(self, stream=None):
+        """Without `stream`: wait for the host copies; with it: order it after them."""
+        L.check(lib.irt_session_host_sync(self.handle, stream), self.ctx.handle, "host sync")
+
     def buffer_ptr(self, which):
         p, n = C.c_void_p(), C.c_uint64()
         L.check(lib.irt_session_buffer(self.handle, which, C.byref(p), C.byref(n)), self.ctx.handle, "buffer")
