@@ -115,7 +115,7 @@ __device__ __forceinline__ Dist scene_distance_cached(const DevScene& sc, const 
     return r;
 }
 
-__global__ void __launch_bounds__(128, 6) march_kernel(const __grid_constant__ irt_frame f, const DevScene sc,
+__global__ void __launch_bounds__(128, 8) march_kernel(const __grid_constant__ irt_frame f, const DevScene sc,
                                                     const float4* __restrict__ march_scene, uint32_t scene_vec4,
                                                     const Grid grid, const RayRecord* __restrict__ rays,
                                                     uint32_t* counters, float* __restrict__ vis) {
@@ -134,7 +134,10 @@ __global__ void __launch_bounds__(128, 6) march_kernel(const __grid_constant__ i
 
     bool active = false;
     bool exhausted = false;  // warp-uniform: the queue has no rays left
-    uint32_t phase = kClear, slot = 0;
+    // A lane keeps its ray's index and re-reads the record's target, endpoint
+    // normal and output slot where a phase needs them (L1/L2 hits), which
+    // keeps fewer values live across the distance query.
+    uint32_t phase = kClear, ridx = 0;
     MarchState m;
     m.closest = kNone;
     m.origin = V3{0.f, 0.f, 0.f};  // surface point until the clearance query
@@ -143,8 +146,6 @@ __global__ void __launch_bounds__(128, 6) march_kernel(const __grid_constant__ i
     m.result = 1.f;
     m.previous = 1e20f;
     m.step = 0;
-    V3 target{0.f, 0.f, 0.f}, endn{0.f, 0.f, 0.f};
-
     for (;;) {
         if (!exhausted) {
             unsigned need = __ballot_sync(full, !active);
@@ -159,12 +160,10 @@ __global__ void __launch_bounds__(128, 6) march_kernel(const __grid_constant__ i
                     uint32_t idx = base + (uint32_t)__popc(need & ((1u << lane) - 1u));
                     if (idx < n_rays) {
                         const float4* r = reinterpret_cast<const float4*>(rays + idx);
-                        float4 a = __ldg(r), b = __ldg(r + 1), c = __ldg(r + 2), d = __ldg(r + 3);
+                        float4 a = __ldg(r), b = __ldg(r + 1);
                         m.origin = V3{a.x, a.y, a.z};
-                        slot = __float_as_uint(a.w);
                         m.dir = V3{b.x, b.y, b.z};
-                        target = V3{c.x, c.y, c.z};
-                        endn = V3{d.x, d.y, d.z};
+                        ridx = idx;
                         phase = kClear;
                         active = true;
                     }
@@ -174,7 +173,8 @@ __global__ void __launch_bounds__(128, 6) march_kernel(const __grid_constant__ i
         if (!__any_sync(full, active)) break;
         if (!active) continue;
 
-        V3 q = phase == kClear ? m.origin : (phase == kEndpoint ? target : march_point(m));
+        const float4* rec = reinterpret_cast<const float4*>(rays + ridx);
+        V3 q = phase == kClear ? m.origin : (phase == kEndpoint ? xyz(__ldg(rec + 2)) : march_point(m));
         uint32_t hint = phase == kMarch ? m.closest : kNone;
         Dist d = scene_distance_cached(sc, f, grid, nodes, objs, q, hint, phase != kMarch);
 
@@ -182,21 +182,23 @@ __global__ void __launch_bounds__(128, 6) march_kernel(const __grid_constant__ i
         if (phase == kClear) {
             m.closest = d.closest;
             m.origin = m.origin + m.dir * clearance_epsilon(eps, d.voxel);
+            const V3 endn = xyz(__ldg(rec + 3));
             if (dot(endn, endn) > .5f) {
                 phase = kEndpoint;
             } else {
                 phase = kMarch;
-                out = march_begin(m, target, eps, max_steps);
+                out = march_begin(m, xyz(__ldg(rec + 2)), eps, max_steps);
             }
         } else if (phase == kEndpoint) {
             phase = kMarch;
+            const V3 target = xyz(__ldg(rec + 2)), endn = xyz(__ldg(rec + 3));
             out = march_begin(m, target + endn * clearance_epsilon(eps, d.voxel), eps, max_steps);
         } else {
             m.closest = d.closest;
             out = march_after(m, d.best, eps, f.sdf[2], max_steps);
         }
         if (out >= 0.f) {
-            vis[slot] = out;
+            vis[__float_as_uint(__ldg(rec).w)] = out;
             active = false;
         }
     }
