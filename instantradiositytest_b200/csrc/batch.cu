@@ -176,6 +176,7 @@ SvgfLaunch svgf_base(irt_session* s, const irt_gbuffer& g) {
     L.old_normal = s->prev_normal;
     L.guide = s->guide[0];
     L.old_guide = s->guide[1];
+    L.feat = s->feat;
     L.radiance_f16 = s->desc.radiance_format == IRT_RADIANCE_F16;
     L.moments_f16 = s->desc.moments_format == IRT_MOMENTS_F16;
     return L;
@@ -248,9 +249,10 @@ irt_status build_tables(irt_batch* b, int p, irt_scene* const* scenes, const irt
             }
             irt_svgf_view_fill(A, hs[2 + i].data() + sv * v);
         }
-        SvgfLaunch G0 = S;  // positions of this frame
+        SvgfLaunch G0 = S;  // positions and edge-stopping features of this frame
         G0.in = g[v].depth;
         G0.out = s->guide[0];
+        G0.out2 = s->feat;
         irt_svgf_view_fill(G0, hs[6].data() + sv * v);
         SvgfLaunch G1 = S;  // positions of the previous frame's pixels
         G1.in = s->prev_depth;
@@ -398,7 +400,9 @@ irt_status launch_frame(irt_batch* b, int p, cudaStream_t st, const int shape_of
        "batch frames");
     mark(1);
     for (size_t w = 0; w < waves; w++) {
-        CK(irt_launch_svgf_batched(batch_launch(b, w, t.sviews[6], sv, -1), 3, st), "batch guides");
+        CK(irt_launch_svgf_batched(batch_launch(b, w, t.sviews[6], sv, -1),
+                                   b->desc.gbuffer_format == IRT_GBUFFER_F32 ? 3 : 6, st),
+           "batch guides");
         CK(irt_launch_svgf_batched(batch_launch(b, w, t.sviews[7], sv, -1), 4, st), "batch previous guides");
         mark(2);
         CK(irt_launch_lighting_batched(batch_launch(b, w, t.largs, la, -1), kStageArchive, st), "batch archive");

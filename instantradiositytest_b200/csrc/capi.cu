@@ -362,6 +362,7 @@ uint64_t irt_session_bytes(const irt_session_desc* d) {
     b += 16;           // error word
     if (d->fused == 1) b += P * (2 * sizeof(RayRecord) + 2 * 4 + 2 * 16) + 16;  // ray queue, vis, pending
     b += P * 16 * 2;                                                             // position guides
+    b += P * 32;                                                                 // SVGF features
     return b;
 }
 
@@ -439,6 +440,7 @@ irt_status irt_session_create(irt_context* ctx, const irt_session_desc* desc, ir
     for (int k = 0; k < 2; k++) {
         if (!st) st = dev_alloc(ctx, &s->guide[k], P * 16, used);
     }
+    if (!st) st = dev_alloc(ctx, &s->feat, P * 32, used);
     if (!st && cudaDeviceGetAttribute(&s->num_sms, cudaDevAttrMultiProcessorCount, ctx->device) != cudaSuccess)
         st = IRT_E_CUDA;
     if (st) return fail(st);
@@ -452,7 +454,7 @@ void irt_session_destroy(irt_session* s) {
     void* ptrs[] = {s->dres[0], s->dres[1], s->dres[2], s->ires[0], s->ires[1], s->ires[2], s->archive,
                     s->prev_depth, s->prev_normal, s->direct, s->noisy, s->moments[0], s->moments[1],
                     s->feedback[0], s->feedback[1], s->temporal, s->scratch[0], s->scratch[1], s->filtered, s->error,
-                    s->rays, s->ray_counters, s->vis, s->pending, s->guide[0], s->guide[1]};
+                    s->rays, s->ray_counters, s->vis, s->pending, s->guide[0], s->guide[1], s->feat};
     for (void* p : ptrs)
         if (p) cudaFree(p);
     if (s->pipe.ready) {
@@ -499,7 +501,10 @@ static cudaError_t compute_guides(irt_session* s, const irt_frame* f, const irt_
     G.old_depth = s->prev_depth;
     G.old_normal = s->prev_normal;
     G.out = s->guide[0];
-    cudaError_t e = irt_launch_svgf(G, 3, st);
+    G.out2 = s->feat;
+    G.radiance_f16 = s->desc.radiance_format == IRT_RADIANCE_F16;
+    // positions, and for decoded G-buffer formats the edge-stopping features
+    cudaError_t e = irt_launch_svgf(G, s->desc.gbuffer_format == IRT_GBUFFER_F32 ? 3 : 6, st);
     if (e != cudaSuccess) return e;
     G.out = s->guide[1];
     e = irt_launch_svgf(G, 4, st);
@@ -654,6 +659,7 @@ irt_status irt_frame_svgf(irt_session* s, const irt_frame* f, const irt_gbuffer*
         L.old_normal = s->prev_normal;
         L.guide = s->guide[0];
         L.old_guide = s->guide[1];
+        L.feat = s->feat;
         L.radiance_f16 = s->desc.radiance_format == IRT_RADIANCE_F16;
         L.moments_f16 = s->desc.moments_format == IRT_MOMENTS_F16;
         L.in = s->noisy;

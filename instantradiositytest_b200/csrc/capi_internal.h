@@ -97,6 +97,7 @@ struct irt_session {
     // per-pixel world positions: [0] this frame, [1] the previous frame's
     // pixels from the previous depth and previous_inv_vp
     float4* guide[2] = {nullptr, nullptr};
+    float4* feat = nullptr;  // this frame's SVGF edge-stopping features, 2 float4 per pixel
     uint32_t guide_frame = 0xffffffffu;
     int num_sms = 0;
     // Host-input pipeline (irt_render_frame_host), created on first use:

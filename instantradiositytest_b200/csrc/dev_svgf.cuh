@@ -1,6 +1,8 @@
 // dev_svgf.cuh — shared helpers of the SVGF kernels (svgf.wgsl:18-44, :90):
 // history test, per-pixel guides and the edge-stopping geometry weight.
 #pragma once
+#include <type_traits>
+
 #include "dev_common.cuh"
 #include "kernels.h"
 
@@ -16,6 +18,11 @@ struct SvgfCtx {
     // same values.
     const float4* guide;
     const float4* old_guide;
+    // Per-pixel edge-stopping features of this frame (feature_kernel), two
+    // float4 per pixel: (normal, roughness), (colour, metal) — the decoded
+    // G-buffer values a tap reads, in 2 loads instead of 4 plane reads and
+    // decodes; null to read the planes.  Requires `guide`.
+    const float4* feat;
 };
 
 // x^64 as six squarings (the `pow(max(dot, 0), 64)` normal weight).
@@ -71,6 +78,8 @@ struct MomF16 {
 
 template <class G>
 struct Sv {
+    // Feature records are read for G-buffer formats that decode per tap.
+    static constexpr bool kFeatures = !std::is_same<G, GbF32>::value;
     const irt_frame& f;
     const SvgfCtx<G>& c;
     int32_t W, H;
@@ -101,6 +110,18 @@ struct Sv {
     __device__ __forceinline__ Guide guide(int32_t x, int32_t y) const {
         Guide a;
         size_t i = idx(x, y);
+        if constexpr (kFeatures) {
+            if (c.feat) {
+                const float4 g = __ldg(c.guide + i), n = __ldg(c.feat + 2 * i), k = __ldg(c.feat + 2 * i + 1);
+                a.position = xyz(g);
+                a.normal = xyz(n);
+                a.color = xyz(k);
+                a.m0 = n.w;
+                a.m1 = k.w;
+                a.pixel_scale = g.w;  // distance(position, camera) / height (guide_kernel)
+                return a;
+            }
+        }
         a.position = position(x, y);
         a.normal = c.g.n(i);
         a.color = c.g.c(i);
@@ -114,6 +135,20 @@ struct Sv {
     __device__ __forceinline__ float geometry_weight(const Guide& a, int32_t qx, int32_t qy, float stride) const {
         if (!inside(qx, qy)) return 0.f;
         size_t q = idx(qx, qy);
+        if constexpr (kFeatures) {
+            if (c.feat) {
+                const float4 g = __ldg(c.guide + q);
+                if (g.w < 0.f) return 0.f;  // depth >= 1
+                const float4 n = __ldg(c.feat + 2 * q), k = __ldg(c.feat + 2 * q + 1);
+                float wn = pow64(wmax(dot(a.normal, xyz(n)), 0.f));
+                float tolerance = wmax(.0001f, a.pixel_scale * stride * .5f);
+                float wz = expf(-fabsf(dot(xyz(g) - a.position, a.normal)) / tolerance);
+                V3 dc = a.color - xyz(k);
+                float d0 = a.m0 - n.w, d1 = a.m1 - k.w;
+                float wc = expf(-length(dc) * 8.f - sqrtf(d0 * d0 + d1 * d1) * 8.f);
+                return wn * wz * wc;
+            }
+        }
         float dq = c.g.d(q);
         if (dq >= 1.f) return 0.f;
         V3 nq = c.g.n(q);
@@ -197,6 +232,9 @@ __host__ inline SvgfCtx<G> make_ctx(const SvgfLaunch& L) {
     c.old_normal = reinterpret_cast<const typename G::NormalT*>(L.old_normal);
     c.guide = L.guide;
     c.old_guide = L.old_guide;
+    // Feature records pay off where a tap would decode (F16, packed); an F32
+    // tap reads the planes as they are.
+    c.feat = (L.guide && !std::is_same<G, GbF32>::value) ? L.feat : nullptr;
     return c;
 }
 

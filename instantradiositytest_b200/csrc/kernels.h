@@ -110,10 +110,12 @@ struct SvgfLaunch {
     int moments_f16;          // moments: 0 float4 (E[l], E[l^2], age, 0); 1 MomF16 (half mean, half deviation, f32 age)
     const float4* guide;      // per-pixel positions of this frame (or null)
     const float4* old_guide;  // ... of the previous frame (or null)
+    const float4* feat;       // per-pixel edge-stopping features (or null)
 };
 // irt_launch_svgf stages: 0 temporal, 1 variance, 2 a-trous, 3 position guide
 // of this frame (out = float4[W*H]), 4 guide of the previous frame (from
-// old_depth and previous_inv_vp).
+// old_depth and previous_inv_vp), 6 guide of this frame (out) and its
+// edge-stopping features (out2 = float4[2*W*H]).
 
 // VPL paths of one frame (vplgen.cu): lights on the device, ray casts
 // against a workload's analytic primitive table.
@@ -153,7 +155,7 @@ void irt_lighting_args_fill(const LightingLaunch& L, void* out);
 cudaError_t irt_launch_lighting_batched(const BatchLaunch& B, int stage, cudaStream_t st);
 // SVGF stages of a batch: 0 temporal, 1 variance, 2 a-trous (records carry
 // the step), 3 guides of this frame, 4 guides of the previous frame, 5 depth
-// and normal history copy.
+// and normal history copy, 6 guides and features of this frame.
 size_t irt_svgf_view_size(int gbuffer_format);
 void irt_svgf_view_fill(const SvgfLaunch& L, void* out);
 cudaError_t irt_launch_svgf_batched(const BatchLaunch& B, int stage, cudaStream_t st);

@@ -166,6 +166,24 @@ __global__ void __launch_bounds__(256) guide_kernel(const __grid_constant__ irt_
     guide_body(f, depth, previous, out, (size_t)blockIdx.x * blockDim.x + threadIdx.x);
 }
 
+// Guide of this frame and the decoded edge-stopping features of every pixel:
+// feat[2i] = (normal, roughness), feat[2i+1] = (colour, metal).
+template <class G>
+__device__ __forceinline__ void feature_body(const irt_frame& f, const G& g, float4* guide, float4* feat, size_t i) {
+    guide_body(f, g.depth, 0, guide, i);
+    if (i >= (size_t)f.size[0] * f.size[1]) return;
+    V3 n = g.n(i), c = g.c(i);
+    float2 pm = g.pm(i);
+    feat[2 * i] = make_float4(n.x, n.y, n.z, pm.x);
+    feat[2 * i + 1] = make_float4(c.x, c.y, c.z, pm.y);
+}
+
+template <class G>
+__global__ void __launch_bounds__(256) feature_kernel(const __grid_constant__ irt_frame f, const __grid_constant__ G g,
+                                                      float4* guide, float4* feat) {
+    feature_body<G>(f, g, guide, feat, (size_t)blockIdx.x * blockDim.x + threadIdx.x);
+}
+
 // Batched guides (in = depth, out = guide) and depth/normal history copy
 // (in = depth, aux = normal, out = previous depth, out2 = previous normal);
 // 1-D tiles of 256 pixels.
@@ -176,6 +194,16 @@ __global__ void __launch_bounds__(256) guide_batched(const irt_frame* __restrict
     const SView<G>& w = views[v];
     guide_body(frames[v], (const float*)w.in, previous, (float4*)w.out,
                (size_t)(blockIdx.x - __ldg(tile_start + v)) * blockDim.x + threadIdx.x);
+}
+
+template <class G>
+__global__ void __launch_bounds__(256) feature_batched(const irt_frame* __restrict__ frames,
+                                                       const SView<G>* __restrict__ views,
+                                                       const uint32_t* __restrict__ tile_start, uint32_t n) {
+    const uint32_t v = svgf_find_view(tile_start, n, blockIdx.x);
+    const SView<G>& w = views[v];
+    feature_body<G>(frames[v], w.c.g, (float4*)w.out, (float4*)w.out2,
+                    (size_t)(blockIdx.x - __ldg(tile_start + v)) * blockDim.x + threadIdx.x);
 }
 
 template <class G>
@@ -210,6 +238,10 @@ static cudaError_t svgf_typed(const SvgfLaunch& L, int stage, cudaStream_t st) {
         guide_kernel<<<(unsigned)((P + 255) / 256), 256, 0, st>>>(f, stage == 3 ? L.gbuffer.depth : L.old_depth,
                                                                    stage == 4, (float4*)L.out);
     } break;
+    case 6: {
+        size_t P = (size_t)f.size[0] * f.size[1];
+        feature_kernel<G><<<(unsigned)((P + 255) / 256), 256, 0, st>>>(f, c.g, (float4*)L.out, (float4*)L.out2);
+    } break;
     default: return cudaErrorInvalidValue;
     }
     return cudaGetLastError();
@@ -223,6 +255,7 @@ static cudaError_t svgf_batched_typed(const BatchLaunch& B, int stage, cudaStrea
     case 3:
     case 4: guide_batched<G><<<B.tiles, 256, 0, st>>>(B.frames, views, B.tile_start, B.n, stage == 4); break;
     case 5: history_batched<G><<<B.tiles, 256, 0, st>>>(B.frames, views, B.tile_start, B.n); break;
+    case 6: feature_batched<G><<<B.tiles, 256, 0, st>>>(B.frames, views, B.tile_start, B.n); break;
     default: return cudaErrorInvalidValue;
     }
     return cudaGetLastError();
@@ -281,6 +314,14 @@ cudaError_t irt_launch_svgf(const SvgfLaunch& L, int stage, cudaStream_t st) {
     if (stage == 1 || stage == 2) return irt_launch_svgf_spatial(L, stage, st);
     if (stage == 3 || stage == 4)  // guides read neither radiance nor moments
         return svgf_typed<GbF32, RadF32, MomF32>(L, stage, st);
+    if (stage == 6) {  // features read the G-buffer format only
+        SvgfLaunch F = L;
+        F.radiance_f16 = 0;
+        F.moments_f16 = 0;
+        return dispatch_svgf(F, [&](auto g, auto, auto) {
+            return svgf_typed<decltype(g), RadF32, MomF32>(F, stage, st);
+        });
+    }
     return dispatch_svgf(L, [&](auto g, auto r, auto m) {
         return svgf_typed<decltype(g), decltype(r), decltype(m)>(L, stage, st);
     });
