@@ -86,6 +86,21 @@ def test_mixed_precision_storage(cuda):
         assert stats[f"f64_{k}"] <= max(RADIANCE_BAR, 1.5 * stats[f"floor_{k}"]), k
 
 
+@pytest.mark.parametrize("debug", [1, 2, 3, 4, 5])
+@pytest.mark.parametrize("schedule", [1, 0])
+def test_debug_views_lockstep_parity(cuda, debug, schedule):
+    """The renderer's debug views (lighting.wgsl:106-134 gates: 1 direct only,
+    2 indirect only, 3 albedo, 4 normals, 5 motion; src/svgf.rs:154-161
+    bypasses SVGF from 3 on) against the oracle."""
+    wl = Workload(0, width=96, height=64)
+    ls = Lockstep(wl, fused=schedule)
+    rows = [ls.frame(i, debug=debug) for i in range(4)]
+    ls.close()
+    stats = summarize(rows)
+    print("debug", debug, "schedule", schedule, stats)
+    check(stats, f"debug {debug}")
+
+
 def test_free_running_images_stay_within_bar(cuda):
     wl = Workload(0)
     ls = Lockstep(wl)
