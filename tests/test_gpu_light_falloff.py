@@ -72,3 +72,64 @@ def test_inverse_square_and_spot_cone(cuda):
     spot_out = centre_radiance(ctx, wl, f, obj, nodes, light(2.5, spot=True, toward=False), planes)
     assert spot_out == 0.0
     ctx.close()
+
+
+def _world_aabb(model16, lo, hi):
+    """World AABB of the SDF-bounds corners under a column-major model (f32,
+    the arithmetic of Workload::frame_data / src/renderer.rs:388-400)."""
+    m = np.asarray(model16, np.float32)
+    pts = []
+    for c in range(8):
+        p = [hi[0] if c & 1 else lo[0], hi[1] if c & 2 else lo[1], hi[2] if c & 4 else lo[2]]
+        pts.append([np.float32(m[a] * np.float32(p[0]) + m[4 + a] * np.float32(p[1]) + m[8 + a] * np.float32(p[2]) +
+                               m[12 + a]) for a in range(3)])
+    pts = np.array(pts, np.float32)
+    return pts.min(0), pts.max(0)
+
+
+def test_moving_occluder_updates_the_hierarchy(cuda):
+    """src/gpu_tests.rs:319-352: moving a uniformly scaled object into the
+    light ray darkens the point — the BVH, the march records and the
+    leaf-order cache follow the objects."""
+    wl = Workload(0, width=64, height=64)
+    ctx = Context()
+    f, obj, nodes, lights = wl.frame(0)
+    planes = wl.gbuffer_cpu(f, L.GBUFFER_F32)
+    inv = np.array(f.inv_vp.m, np.float64).reshape(4, 4).T
+    hp = inv @ np.array([(32 + 0.5) / 64 * 2 - 1, 1 - (32 + 0.5) / 64 * 2, planes["depth"][32, 32], 1.0])
+    p = hp[:3] / hp[3]
+    n = planes["normal"][32, 32][:3].astype(np.float64)
+    n /= np.linalg.norm(n)
+    light = np.zeros((), L.LIGHT_DTYPE)
+    light["position_strength"] = (*(p + n * 2.5), 5.0)
+    light["color_type"] = (1.0, 1.0, 1.0, 0.0)
+    lit = centre_radiance(ctx, wl, f, obj, nodes, light, planes)
+    assert lit > 0
+    # move the last object (a sphere) to the middle of the ray, scaled by 0.25
+    k = len(obj) - 1
+    mesh, material = int(obj["info"][k, 0]), int(obj["info"][k, 1])
+    lo, hi = wl.meshes[mesh]["lo"][:3].copy(), wl.meshes[mesh]["hi"][:3].copy()
+    mid = p + n * 1.25
+    model = L.Mat4()
+    vals = [0.25, 0, 0, 0, 0, 0.25, 0, 0, 0, 0, 0.25, 0, mid[0], mid[1], mid[2], 1.0]
+    for i, x in enumerate(vals):
+        model.m[i] = x
+    moved = obj.copy()
+    rec = np.zeros(1, L.OBJECT_DTYPE)
+    L.lib.irt_pack_object(C.byref(model), C.byref(model), mesh, material, (C.c_float * 3)(*lo), (C.c_float * 3)(*hi),
+                          int(wl.meshes[mesh]["field"][3]), L.ptr(rec))
+    moved[k] = rec[0]
+    los, his = [], []
+    for i in range(len(moved)):
+        mi = int(moved["info"][i, 0])
+        a, b = _world_aabb(moved["model"][i], wl.meshes[mi]["lo"][:3], wl.meshes[mi]["hi"][:3])
+        los.append(a)
+        his.append(b)
+    los = np.ascontiguousarray(np.array(los, np.float32))
+    his = np.ascontiguousarray(np.array(his, np.float32))
+    new_nodes = np.zeros(2 * len(moved) - 1, L.NODE_DTYPE)
+    assert L.lib.irt_build_hierarchy(L.ptr(los), L.ptr(his), len(moved), L.ptr(new_nodes)) == L.IRT_OK
+    dark = centre_radiance(ctx, wl, f, moved, new_nodes, light, planes)
+    print("lit", lit, "occluded", dark)
+    assert dark == 0.0
+    ctx.close()
