@@ -105,6 +105,8 @@ def parse():
     ap.add_argument("--height", type=int, default=0)
     ap.add_argument("--schedule", type=int, default=1, choices=[0, 1, 2],
                     help="1 ray-queue march (default), 2 fused with the march inline, 0 one kernel per entry point")
+    ap.add_argument("--scene", default="", help="a scene manifest (scene.json) to render instead of the "
+                    "procedural room of --config; size from --width/--height (default 1920x1080)")
     ap.add_argument("--no-e2e", action="store_true")
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--cpu-seconds", type=float, default=15.0, help="CPU work budget of the cpu_baseline sample")
@@ -142,12 +144,37 @@ def workload_spec(args):
     over = {}
     if args.width:
         over["width"] = args.width
+    elif args.scene:
+        over["width"] = 1920
     if args.height:
         over["height"] = args.height
+    elif args.scene:
+        over["height"] = 1080
     return preset_spec(args.config, **over)
 
 
-def describe(spec, frames, schedule, storage):
+def make_workload(spec, scene=""):
+    """The procedural room of `spec`, or the scene file `scene` at the
+    spec's size, VPL paths and SDF texel format."""
+    from instantradiositytest_b200.workload import Workload
+
+    if not scene:
+        return Workload(spec)
+    return Workload.load(scene, width=spec.width, height=spec.height, vpl_count=spec.vpl_count,
+                         vpl_bounces=spec.vpl_bounces, sdf_format=spec.sdf_format)
+
+
+def describe(spec, frames, schedule, storage, scene=None):
+    if scene is not None:
+        res = sorted({int(m["field"][3]) for m in scene.meshes})
+        d = describe(spec, frames, schedule, storage)
+        d.update({"workload": f"scene file {os.path.basename(os.path.dirname(os.path.abspath(scene.path)))}"
+                              f"/scene.json: {scene.mesh_count} triangle meshes, {scene.object_count} objects, "
+                              f"{scene.light_count} lights, {spec.width}x{spec.height}, {frames} frames",
+                  "meshes": scene.mesh_count, "objects": scene.object_count, "emitters": scene.light_count,
+                  "sdf": f"{'/'.join(map(str, res))}^3 {'f16' if spec.sdf_format else 'f32'}",
+                  "l2": "a distinct G-buffer per frame"})
+        return d
     return {
         "workload": f"room of {6 if not spec.room_single_mesh else 1}+{spec.n_boxes}+{spec.n_spheres} meshes, "
                     f"{spec.width}x{spec.height}, {frames} frames",
@@ -284,14 +311,14 @@ def ncu_traffic(kernel, workload):
 
 
 # ------------------------------------------------------------------ CPU legs
-def cpu_run(spec, steps, warmup, budget_s, threads=0):
+def cpu_run(spec, steps, warmup, budget_s, threads=0, scene=""):
     """Time the oracle (FP32 restatement of the WGSL) on a band of rows of the
     workload: frames 0..warmup-1 untimed, then `steps` timed frames.  The band
     height is chosen from a probe so the whole run stays near budget_s."""
     from instantradiositytest_b200.workload import Workload
     from oracle import Oracle, OracleScene
 
-    wl = Workload(spec)
+    wl = make_workload(spec, scene)
     W, H = wl.width, wl.height
     orc = Oracle(W, H, wl.settings.vpl_count, wl.settings.restir_max_history, 0, False, threads)
     prev = None
@@ -347,15 +374,16 @@ def reference_arm(args):
                                                               "CPU restatement is timed on the plain configs 0-2"}))
         return
     spec = workload_spec(args)
-    r = cpu_run(spec, args.steps, args.warmup, args.reference_seconds)
+    r = cpu_run(spec, args.steps, args.warmup, args.reference_seconds, scene=args.scene)
     frames = args.steps + args.warmup
     line = {
         "metric": "Mpix-frames/s", "value": r["value"], "unit": "Mpix-frames/s", "n_gpus": args.gpus,
         "steps": args.steps, "warmup": args.warmup, "ms_per_step": 1000.0 * r["seconds"] / r["steps"],
-        "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f32", "data": "synthetic",
+        "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f32", "data": "scene file" if args.scene else "synthetic",
         "impl": "reference",
         "config": describe(spec, frames, "CPU restatement of the WGSL passes (oracle/), OpenMP over pixels",
-                           "f32 throughout (the oracle's arithmetic); f16 SDF texels dequantised"),
+                           "f32 throughout (the oracle's arithmetic); f16 SDF texels dequantised",
+                           make_workload(spec, args.scene) if args.scene else None),
         "cpu_baseline": {"value": r["value"], "unit": "Mpix-frames/s", "cores": r["threads"], "kind": "port",
                          "sample": r["sample"]},
         "e2e": {"value": r["value"], "unit": "Mpix-frames/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
@@ -387,7 +415,7 @@ def ours(args):
         torch.cuda.set_device(0)
     dev = torch.cuda.current_device()
     spec = workload_spec(args)
-    wl = Workload(spec)
+    wl = make_workload(spec, args.scene)
     W, H, P = wl.width, wl.height, wl.width * wl.height
     K, Wm = args.steps, args.warmup
     n_frames = K + Wm
@@ -504,11 +532,11 @@ def ours(args):
     cpu, counters = None, None
     if rank == 0:
         if world == 1 and not args.no_cpu_baseline:
-            r = cpu_run(spec, 1, 1, args.cpu_seconds)
+            r = cpu_run(spec, 1, 1, args.cpu_seconds, scene=args.scene)
             cpu = {"value": r["value"], "unit": "Mpix-frames/s", "cores": r["threads"], "kind": "port",
                    "sample": r["sample"]}
         else:
-            r = cpu_run(spec, 1, 1, 1.0)
+            r = cpu_run(spec, 1, 1, 1.0, scene=args.scene)
         counters = r["counters_per_pixel"]
 
     # ---- roofline of the dominant kernel
@@ -539,8 +567,9 @@ def ours(args):
         line = {
             "metric": "Mpix-frames/s", "value": value, "unit": "Mpix-frames/s", "n_gpus": world, "steps": K,
             "warmup": Wm, "ms_per_step": ms_max / K, "higher_is_better": True, "scaling": "weak",
-            "vs_baseline": None, "dtype": "f32", "data": "synthetic",
-            "config": describe(spec, n_frames, {1: "ray-queue", 2: "fused-inline", 0: "plain"}[schedule], storage),
+            "vs_baseline": None, "dtype": "f32", "data": "scene file" if args.scene else "synthetic",
+            "config": describe(spec, n_frames, {1: "ray-queue", 2: "fused-inline", 0: "plain"}[schedule], storage,
+                               wl if args.scene else None),
             "p50_frame_ms": float(np.percentile(frame_ms, 50)), "p99_frame_ms": float(np.percentile(frame_ms, 99)),
             "stage_ms": {n: float(mean_ms[i]) for i, n in enumerate(names)},
             "roofline": roofline, "cpu_baseline": cpu, "e2e": e2e,

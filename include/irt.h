@@ -393,7 +393,21 @@ irt_status irt_workload_frame(irt_workload* wl, uint32_t index, uint32_t debug, 
 irt_status irt_workload_gbuffer_cpu(const irt_workload* wl, const irt_frame* frame,
                                     const irt_object* objects, int32_t format, float* depth,
                                     void* normal, void* color, void* params, void* motion);
-/* CPU VPL generator: vpl.wgsl:1-47 with analytic ray casts. */
+/* Scene-format loader: Scene::load + Scene::validate (src/scene.rs:157-382)
+ * of the version-1 manifest at `manifest_path` and the binaries it names
+ * (paths relative to the manifest's directory): meshes as triangle lists
+ * (64-byte vertices, u32 indices) with their SDF fields (res^3 f32), objects,
+ * materials, lights and the fixed camera.  The workload's atlas, mesh rows,
+ * per-frame data and producers then serve the file's scene (triangle casts;
+ * textured materials are rejected).  From `spec` only width, height,
+ * sdf_format, vpl_count and vpl_bounces are used.  On failure returns
+ * IRT_E_INVALID (or IRT_E_NOMEM) and writes the reason, prefixed as the
+ * reference's error context ("reading <path>", "parsing <path>",
+ * "scene <path>", "mesh <id>"), NUL-terminated into error[0..error_len). */
+irt_status irt_workload_load(const char* manifest_path, const irt_workload_spec* spec,
+                             irt_workload** out, char* error, uint64_t error_len);
+/* CPU VPL generator: vpl.wgsl:1-47 with ray casts against the workload's
+ * analytic solids or triangle hierarchies. */
 irt_status irt_workload_vpls_cpu(const irt_workload* wl, const irt_frame* frame,
                                  const irt_object* objects, const irt_light* lights,
                                  irt_vpl* out);
@@ -406,8 +420,9 @@ irt_status irt_gbuffer_render(irt_context* ctx, const irt_workload* wl, const ir
  * its dispatch in src/renderer.rs:1873-1884): frame->counts[1] paths of up to
  * frame->counts[2] bounces from the lights last uploaded to `scene`
  * (irt_scene_update), written to the device pool `out`.  Ray casts run
- * against the workload's analytic primitives (the reference uses a hardware
- * ray query against its TLAS).  Same contract as irt_workload_vpls_cpu. */
+ * against the workload's primitives: analytic solids or the triangle
+ * hierarchies of a loaded scene (the reference uses a hardware ray query
+ * against its TLAS).  Same contract as irt_workload_vpls_cpu. */
 irt_status irt_vpl_generate(irt_scene* scene, const irt_workload* wl, const irt_frame* frame,
                             irt_vpl* out, void* stream);
 

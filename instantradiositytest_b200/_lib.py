@@ -192,6 +192,7 @@ _PROTOS = {
                                C.POINTER(C.c_float), U32, P]),
     "irt_workload_preset": (I32, [I32, C.POINTER(WorkloadSpec)]),
     "irt_workload_create": (I32, [C.POINTER(WorkloadSpec), C.POINTER(P)]),
+    "irt_workload_load": (I32, [C.c_char_p, C.POINTER(WorkloadSpec), C.POINTER(P), C.c_char_p, U64]),
     "irt_workload_destroy": (None, [P]),
     "irt_workload_mesh_count": (U32, [P]),
     "irt_workload_object_count": (U32, [P]),

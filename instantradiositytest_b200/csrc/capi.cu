@@ -317,7 +317,7 @@ irt_status irt_vpl_generate(irt_scene* sc, const irt_workload* wl, const irt_fra
     V.frame = f;
     V.lights = sc->lights;
     V.out = out;
-    CK(irt_workload_prims(wl, &V.prims, &V.n_prims), "workload primitives");
+    CK(irt_workload_prims(wl, &V.prims), "workload primitives");
     CK(irt_launch_vpls(V, static_cast<cudaStream_t>(stream)), "vpl kernel");
     return IRT_OK;
 }
@@ -949,9 +949,10 @@ irt_status irt_session_reservoirs(irt_session* s, int32_t domain, int32_t k, voi
 
 void irt_workload_destroy(irt_workload* wl) {
     if (!wl) return;
-    if (wl->w.dev_prims) {
+    if (wl->w.dev_prims || wl->w.dev_nodes || wl->w.dev_tris) {
         DeviceGuard g(wl->w.dev_prims_device);
-        cudaFree(wl->w.dev_prims);
+        for (void* p : {wl->w.dev_prims, wl->w.dev_nodes, wl->w.dev_tris})
+            if (p) cudaFree(p);
     }
     delete wl;
 }

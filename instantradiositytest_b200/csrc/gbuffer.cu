@@ -1,6 +1,7 @@
-// gbuffer.cu — CUDA G-buffer producer: one analytic primary ray per pixel
-// centre against the workload's boxes and spheres (stands in for the
-// gbuffer.wgsl raster; same outputs as irt_workload_gbuffer_cpu, in f32).
+// gbuffer.cu — CUDA G-buffer producer: one primary ray per pixel centre
+// against the workload's primitives (analytic boxes and spheres, or the
+// triangle hierarchies of a loaded scene with back faces culled), standing in
+// for the gbuffer.wgsl raster; same outputs as irt_workload_gbuffer_cpu, in f32.
 #include <cuda_fp16.h>
 #include <cuda_runtime.h>
 
@@ -35,7 +36,7 @@ __device__ __forceinline__ uint32_t oct_snorm16(float x, float y, float z) {
     return ((uint32_t)(uint16_t)(int16_t)qu) | ((uint32_t)(uint16_t)(int16_t)qv << 16);
 }
 
-__global__ void gbuffer_kernel(const __grid_constant__ irt_frame f, const GPrim* prims, uint32_t n_prims, int fmt,
+__global__ void gbuffer_kernel(const __grid_constant__ irt_frame f, const irt::PrimTable T, int fmt,
                                float* depth, void* normal, void* color, void* params, void* motion) {
     uint32_t x = blockIdx.x * blockDim.x + threadIdx.x;
     uint32_t y = blockIdx.y * blockDim.y + threadIdx.y;
@@ -52,10 +53,10 @@ __global__ void gbuffer_kernel(const __grid_constant__ irt_frame f, const GPrim*
     // d spans near to far plane: t in [0, 1).
     float best;
     float nl_best[3] = {0, 0, 0};
-    int hit = irtd::cast_prims(prims, n_prims, o, d, 0.f, 1.f, best, nl_best);
+    int hit = irtd::cast_prims(T, o, d, 0.f, 1.f, true, best, nl_best);
     float dep = 1.f, nrm[3] = {0, 0, 0}, col[3] = {0, 0, 0}, par[2] = {0, 0}, mot[2] = {0, 0};
     if (hit >= 0) {
-        const GPrim& p = prims[hit];
+        const GPrim& p = T.prims[hit];
         float w[4];
         xf(p.model, nl_best[0], nl_best[1], nl_best[2], 0.f, w);
         float inv = 1.f / sqrtf(w[0] * w[0] + w[1] * w[1] + w[2] * w[2]);
@@ -99,8 +100,10 @@ __global__ void gbuffer_kernel(const __grid_constant__ irt_frame f, const GPrim*
 }  // namespace
 
 // Flattened primitive table of a workload on the current device (static
-// scenes: built once and kept with the workload).
-cudaError_t irt_workload_prims(const irt_workload* wl_c, const void** prims_out, uint32_t* n_out) {
+// scenes: built once and kept with the workload), with the triangle
+// hierarchies of loaded meshes concatenated into shared node and triangle
+// tables.
+cudaError_t irt_workload_prims(const irt_workload* wl_c, irt::PrimTable* out) {
     irt_workload* wl = const_cast<irt_workload*>(wl_c);
     irt::Workload& w = wl->w;
     int dev = 0;
@@ -108,40 +111,75 @@ cudaError_t irt_workload_prims(const irt_workload* wl_c, const void** prims_out,
     if (e != cudaSuccess) return e;
     if (!w.dev_prims || w.dev_prims_device != dev) {
         std::vector<GPrim> prims;
+        std::vector<irt::TriNode> nodes;
+        std::vector<irt::TriRec> tris;
+        std::vector<uint32_t> node_base(w.mesh_desc.size(), 0), tri_base(w.mesh_desc.size(), 0);
+        for (size_t m = 0; m < w.mesh_desc.size(); m++) {
+            const irt::MeshDesc& md = w.mesh_desc[m];
+            if (!md.triangles) continue;
+            node_base[m] = (uint32_t)nodes.size();
+            tri_base[m] = (uint32_t)tris.size();
+            nodes.insert(nodes.end(), md.bvh.nodes.begin(), md.bvh.nodes.end());
+            tris.insert(tris.end(), md.bvh.tris.begin(), md.bvh.tris.end());
+        }
         for (uint32_t oi = 0; oi < w.objs.size(); oi++) {
             const irt::Obj& ob = w.objs[oi];
             irt_mat4 model = irt::to_f32(ob.model), inv = irt::to_f32(ob.inv_model);
             const irt_material& m = w.materials[ob.material];
-            for (const irt::Part& part : w.mesh_desc[ob.mesh].parts) {
-                GPrim g{};
-                for (int k = 0; k < 16; k++) {
-                    g.inv_model[k] = inv.m[k];
-                    g.model[k] = model.m[k];
+            const irt::MeshDesc& md = w.mesh_desc[ob.mesh];
+            GPrim g{};
+            for (int k = 0; k < 16; k++) {
+                g.inv_model[k] = inv.m[k];
+                g.model[k] = model.m[k];
+            }
+            for (int k = 0; k < 3; k++) g.color[k] = m.color[k];
+            g.params[0] = fminf(fmaxf(m.params[0], .045f), 1.f);
+            g.params[1] = fminf(fmaxf(m.params[1], 0.f), 1.f);
+            g.object = oi;
+            if (md.triangles) {
+                if (md.bvh.nodes.empty()) continue;
+                g.kind = irt::kPrimTriangles;
+                for (int a = 0; a < 3; a++) {
+                    g.lo[a] = md.bvh.nodes[0].lo[a];
+                    g.hi[a] = md.bvh.nodes[0].hi[a];
                 }
+                g.node_base = node_base[ob.mesh];
+                g.tri_base = tri_base[ob.mesh];
+                prims.push_back(g);
+                continue;
+            }
+            for (const irt::Part& part : md.parts) {
                 for (int a = 0; a < 3; a++) {
                     g.lo[a] = part.sphere ? 0.f : (float)part.lo[a];
                     g.hi[a] = part.sphere ? 0.f : (float)part.hi[a];
                 }
                 if (part.sphere) g.lo[0] = (float)part.radius;
-                for (int k = 0; k < 3; k++) g.color[k] = m.color[k];
-                g.params[0] = fminf(fmaxf(m.params[0], .045f), 1.f);
-                g.params[1] = fminf(fmaxf(m.params[1], 0.f), 1.f);
-                g.object = oi;
-                g.sphere = part.sphere ? 1u : 0u;
+                g.kind = part.sphere ? irt::kPrimSphere : irt::kPrimBox;
                 prims.push_back(g);
             }
         }
-        if (w.dev_prims) cudaFree(w.dev_prims);
-        w.dev_prims = nullptr;
-        e = cudaMalloc(&w.dev_prims, prims.size() * sizeof(GPrim));
-        if (e != cudaSuccess) return e;
-        e = cudaMemcpy(w.dev_prims, prims.data(), prims.size() * sizeof(GPrim), cudaMemcpyHostToDevice);
+        for (void** p : {&w.dev_prims, &w.dev_nodes, &w.dev_tris}) {
+            if (*p) cudaFree(*p);
+            *p = nullptr;
+        }
+        w.dev_prims_count = 0;
+        auto upload = [](void** dst, const void* src, size_t bytes) {
+            if (bytes == 0) return cudaSuccess;
+            cudaError_t r = cudaMalloc(dst, bytes);
+            if (r != cudaSuccess) return r;
+            return cudaMemcpy(*dst, src, bytes, cudaMemcpyHostToDevice);
+        };
+        e = upload(&w.dev_prims, prims.data(), prims.size() * sizeof(GPrim));
+        if (e == cudaSuccess) e = upload(&w.dev_nodes, nodes.data(), nodes.size() * sizeof(irt::TriNode));
+        if (e == cudaSuccess) e = upload(&w.dev_tris, tris.data(), tris.size() * sizeof(irt::TriRec));
         if (e != cudaSuccess) return e;
         w.dev_prims_device = dev;
         w.dev_prims_count = (uint32_t)prims.size();
     }
-    *prims_out = w.dev_prims;
-    *n_out = w.dev_prims_count;
+    out->prims = static_cast<const GPrim*>(w.dev_prims);
+    out->n = w.dev_prims_count;
+    out->nodes = static_cast<const irt::TriNode*>(w.dev_nodes);
+    out->tris = static_cast<const irt::TriRec*>(w.dev_tris);
     return cudaSuccess;
 }
 
@@ -151,12 +189,11 @@ extern "C" irt_status irt_gbuffer_render(irt_context* ctx, const irt_workload* w
     (void)objects;
     if (!ctx || !wl || !f || !depth || !normal || !color || !params || !motion) return IRT_E_INVALID;
     if (format < IRT_GBUFFER_F32 || format > IRT_GBUFFER_PACKED) return IRT_E_INVALID;
-    const void* prims = nullptr;
-    uint32_t n = 0;
-    if (irt_workload_prims(wl, &prims, &n) != cudaSuccess) return IRT_E_CUDA;
+    irt::PrimTable T{};
+    if (irt_workload_prims(wl, &T) != cudaSuccess) return IRT_E_CUDA;
     dim3 block(32, 8);
     dim3 grid((f->size[0] + 31) / 32, (f->size[1] + 7) / 8);
     gbuffer_kernel<<<grid, block, 0, static_cast<cudaStream_t>(stream)>>>(
-        *f, static_cast<const GPrim*>(prims), n, format, depth, normal, color, params, motion);
+        *f, T, format, depth, normal, color, params, motion);
     return cudaGetLastError() == cudaSuccess ? IRT_OK : IRT_E_CUDA;
 }

@@ -3,6 +3,7 @@
 #include <cuda_runtime.h>
 
 #include "../../include/irt.h"
+#include "workload.h"
 
 // Lighting stages: 0..7 are the reference entry points in schedule order
 // (candidates_direct, candidates_indirect, temporal_direct, temporal_indirect,
@@ -118,18 +119,17 @@ struct SvgfLaunch {
 // edge-stopping features (out2 = float4[2*W*H]).
 
 // VPL paths of one frame (vplgen.cu): lights on the device, ray casts
-// against a workload's analytic primitive table.
+// against a workload's primitive table.
 struct VplLaunch {
     const irt_frame* frame;
-    const void* prims;  // irt::GPrim[n_prims]
-    uint32_t n_prims;
+    irt::PrimTable prims;
     const irt_light* lights;
     irt_vpl* out;
 };
 cudaError_t irt_launch_vpls(const VplLaunch& L, cudaStream_t st);
-// The workload's flattened primitive table on the current device (built on
-// first use and kept with the workload).
-cudaError_t irt_workload_prims(const irt_workload* wl, const void** prims, uint32_t* n);
+// The workload's flattened primitive table and triangle tables on the
+// current device (built on first use and kept with the workload).
+cudaError_t irt_workload_prims(const irt_workload* wl, irt::PrimTable* out);
 
 cudaError_t irt_launch_lighting(const LightingLaunch& L, int stage, cudaStream_t st);
 

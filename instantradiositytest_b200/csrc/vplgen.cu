@@ -5,8 +5,8 @@
 // flux = source flux x path throughput x BSDF weight / path count), then
 // continues with a sampled BSDF direction and Russian roulette between
 // rr.x and rr.y.  The reference traces with a hardware ray query against
-// the scene's acceleration structure; here the ray cast runs against the
-// workload's analytic primitive table (dev_prims.cuh).
+// the scene's acceleration structure (no face culling); here the ray cast
+// runs against the workload's primitive table (dev_prims.cuh).
 #include <cuda_runtime.h>
 
 #include "dev_common.cuh"
@@ -59,8 +59,8 @@ __device__ __forceinline__ void sample_bsdf(const Surface& s, uint32_t& rng, V3&
     weight = brdf(s, wi) * (nl / wmax(pdf, .00001f));
 }
 
-__global__ void __launch_bounds__(128) vpl_kernel(const __grid_constant__ irt_frame f, const irt::GPrim* prims,
-                                                  uint32_t n_prims, const irt_light* lights, irt_vpl* out) {
+__global__ void __launch_bounds__(128) vpl_kernel(const __grid_constant__ irt_frame f, const irt::PrimTable T,
+                                                  const irt_light* lights, irt_vpl* out) {
     const uint32_t id = blockIdx.x * blockDim.x + threadIdx.x;
     const uint32_t n = f.counts[1];
     if (id >= n) return;
@@ -97,12 +97,12 @@ __global__ void __launch_bounds__(128) vpl_kernel(const __grid_constant__ irt_fr
     for (uint32_t bounce = 0; bounce < f.counts[2]; bounce++) {
         float o[3] = {origin.x, origin.y, origin.z}, d[3] = {direction.x, direction.y, direction.z};
         float t, nl[3];
-        int k = cast_prims(prims, n_prims, o, d, .0005f, 10000.f, t, nl);
+        int k = cast_prims(T, o, d, .0005f, 10000.f, false, t, nl);
         if (k < 0) {
             v.flux[0] = v.flux[1] = v.flux[2] = v.flux[3] = 0.f;
             break;
         }
-        const irt::GPrim& p = prims[k];
+        const irt::GPrim& p = T.prims[k];
         float w4[4];
         xf4(p.model, nl[0], nl[1], nl[2], 0.f, w4);
         Surface s;
@@ -149,7 +149,6 @@ __global__ void __launch_bounds__(128) vpl_kernel(const __grid_constant__ irt_fr
 cudaError_t irt_launch_vpls(const VplLaunch& L, cudaStream_t st) {
     const uint32_t n = L.frame->counts[1];
     if (n == 0) return cudaSuccess;
-    irtd::vpl_kernel<<<(n + 127) / 128, 128, 0, st>>>(*L.frame, static_cast<const irt::GPrim*>(L.prims), L.n_prims,
-                                                      L.lights, L.out);
+    irtd::vpl_kernel<<<(n + 127) / 128, 128, 0, st>>>(*L.frame, L.prims, L.lights, L.out);
     return cudaGetLastError();
 }

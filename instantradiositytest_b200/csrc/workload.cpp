@@ -141,7 +141,7 @@ namespace irt {
 
 // Local-space intersection of one object's primitive set.
 bool Workload::intersect_object(uint32_t oi, const double ow[3], const double dw[3], double tmin, double tmax,
-                                double& t, double nw[3]) const {
+                                double& t, double nw[3], bool cull) const {
     const Obj& ob = objs[oi];
     const MeshDesc& md = mesh_desc[ob.mesh];
     double o[4], d[4];
@@ -149,6 +149,7 @@ bool Workload::intersect_object(uint32_t oi, const double ow[3], const double dw
     transform(ob.inv_model, dw[0], dw[1], dw[2], 0.0, d);
     bool hit = false;
     double nl[3];
+    if (md.triangles) hit = cast_tri_bvh(md.bvh, o, d, tmin, tmax, cull, t, nl);
     for (const Part& p : md.parts) {
         double tt, nn[3];
         bool h = p.sphere ? ray_sphere(o, d, p.radius, tmin, tmax, tt, nn)
@@ -173,11 +174,11 @@ bool Workload::intersect_object(uint32_t oi, const double ow[3], const double dw
 }
 
 bool Workload::cast(const double o[3], const double d[3], double tmin, double tmax, double& t, double n[3],
-                    uint32_t& object) const {
+                    uint32_t& object, bool cull) const {
     bool hit = false;
     for (uint32_t i = 0; i < objs.size(); i++) {
         double tt, nn[3];
-        if (intersect_object(i, o, d, tmin, tmax, tt, nn)) {
+        if (intersect_object(i, o, d, tmin, tmax, tt, nn, cull)) {
             tmax = tt;
             t = tt;
             n[0] = nn[0];
@@ -191,6 +192,18 @@ bool Workload::cast(const double o[3], const double d[3], double tmin, double tm
 }
 
 void Workload::camera_at(uint32_t frame, double eye[3], double target[3]) const {
+    if (loaded) {
+        // Fixed camera: eye at its position, looking down its local -z.
+        double q[4] = {cam_q[0], cam_q[1], cam_q[2], cam_q[3]};
+        M4 r = scale_rotation_translation(1.0, q, D3{0, 0, 0});
+        double fwd[4];
+        transform(r, 0, 0, -1, 0, fwd);
+        for (int a = 0; a < 3; a++) {
+            eye[a] = cam_eye[a];
+            target[a] = cam_eye[a] + fwd[a];
+        }
+        return;
+    }
     // Orbit and dolly follow a triangle wave of period 2*kPathFrames so the
     // camera sweeps a fixed sector however many frames are rendered.
     double period = 2.0 * path_frames;
@@ -208,6 +221,14 @@ void Workload::camera_at(uint32_t frame, double eye[3], double target[3]) const 
 }
 
 M4 Workload::view_projection(uint32_t frame) const {
+    if (loaded) {
+        // Camera::matrix (src/scene.rs:119-128): perspective (right-handed,
+        // depth 0..1) times the inverse of the camera's rotation-translation.
+        double q[4] = {cam_q[0], cam_q[1], cam_q[2], cam_q[3]};
+        M4 pose = scale_rotation_translation(1.0, q, D3{cam_eye[0], cam_eye[1], cam_eye[2]});
+        M4 proj = perspective_rh_zo(cam_fov, (double)spec.width / (double)spec.height, cam_near, cam_far);
+        return mul(proj, inverse(pose));
+    }
     double eye[3], target[3];
     camera_at(frame, eye, target);
     M4 view = look_at_rh(D3{eye[0], eye[1], eye[2]}, D3{target[0], target[1], target[2]}, D3{0, 0, 1});
@@ -397,6 +418,7 @@ bool Workload::build() {
     for (int64_t mi = 0; mi < (int64_t)count; mi++) {
         const uint32_t m = (uint32_t)mi;
         MeshDesc& md = mesh_desc[m];
+        md.resolution = res;
         // Exporter SDF conventions (tools/export_scene.py:136-152): padding of
         // two voxels of the vertex-box diagonal, bias of -extent * 2e-6.
         double lo[3] = {1e300, 1e300, 1e300}, hi[3] = {-1e300, -1e300, -1e300};
@@ -437,26 +459,28 @@ bool Workload::build() {
                               (m / (atlas_grid[0] * atlas_grid[1])) * res};
         irt_mesh_metadata(md.vertices.data(), (uint32_t)md.vertices.size(), md.indices.data(),
                           (uint32_t)md.indices.size(), smp.data(), res, md.sdf_lo, md.sdf_hi, origin, &meshes[m]);
-        float scale = 1.f;
-        if (spec.sdf_format == IRT_SDF_F16) {
-            // Per-mesh scale: texels hold value / |voxel diagonal| rounded
-            // toward -inf, so the dequantised field never exceeds the f32 one.
-            scale = meshes[m].grid[3];
-            meshes[m].lo[3] = scale;
-        }
-        for (uint32_t z = 0; z < res; z++)
-            for (uint32_t y = 0; y < res; y++)
-                for (uint32_t x = 0; x < res; x++) {
-                    size_t dst = ((size_t)(origin[2] + z) * atlas_dims[1] + origin[1] + y) * atlas_dims[0] + origin[0] + x;
-                    float v = smp[((size_t)z * res + y) * res + x];
-                    if (spec.sdf_format == IRT_SDF_F16)
-                        atlas16[dst] = f16_bits_round_down(v / scale);
-                    else
-                        atlas32[dst] = v;
-                }
+        store_field(m, smp.data(), res, origin);
     }
     // Static scene: previous transforms equal the current ones.
     return true;
+}
+
+void Workload::store_field(uint32_t m, const float* smp, uint32_t res, const uint32_t origin[3]) {
+    float scale = 1.f;
+    if (spec.sdf_format == IRT_SDF_F16) {
+        scale = meshes[m].grid[3];
+        meshes[m].lo[3] = scale;
+    }
+    for (uint32_t z = 0; z < res; z++)
+        for (uint32_t y = 0; y < res; y++)
+            for (uint32_t x = 0; x < res; x++) {
+                size_t dst = ((size_t)(origin[2] + z) * atlas_dims[1] + origin[1] + y) * atlas_dims[0] + origin[0] + x;
+                float v = smp[((size_t)z * res + y) * res + x];
+                if (spec.sdf_format == IRT_SDF_F16)
+                    atlas16[dst] = f16_bits_round_down(v / scale);
+                else
+                    atlas32[dst] = v;
+            }
 }
 
 void Workload::frame_data(uint32_t index, uint32_t debug, irt_frame* f, irt_object* objects, irt_node* nodes,
@@ -512,7 +536,7 @@ void Workload::frame_data(uint32_t index, uint32_t debug, irt_frame* f, irt_obje
         const Obj& o = objs[i];
         const MeshDesc& md = mesh_desc[o.mesh];
         irt_mat4 model = to_f32(o.model);
-        irt_pack_object(&model, &model, o.mesh, o.material, md.sdf_lo, md.sdf_hi, spec.sdf_resolution, &objects[i]);
+        irt_pack_object(&model, &model, o.mesh, o.material, md.sdf_lo, md.sdf_hi, md.resolution, &objects[i]);
         // World AABB of the transformed SDF bounds corners in f32, like
         // glam's transform_point3 (src/renderer.rs:388-400).
         float l[3] = {INFINITY, INFINITY, INFINITY}, h[3] = {-INFINITY, -INFINITY, -INFINITY};

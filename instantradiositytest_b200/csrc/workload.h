@@ -5,6 +5,7 @@
 
 #include "../../include/irt.h"
 #include "host_math.h"
+#include "tri_bvh.h"
 
 namespace irt {
 
@@ -19,6 +20,11 @@ struct MeshDesc {
     std::vector<irt_vertex> vertices;
     std::vector<uint32_t> indices;
     float sdf_lo[3], sdf_hi[3];
+    uint32_t resolution = 0;  // SDF samples per axis
+    // Meshes of a loaded scene file are triangle lists: ray casts run
+    // against their hierarchy instead of analytic parts.
+    bool triangles = false;
+    TriBvh bvh;
 };
 
 struct Obj {
@@ -38,22 +44,37 @@ struct Workload {
     uint32_t atlas_dims[3] = {0, 0, 0}, atlas_grid[3] = {0, 0, 0};
     uint32_t path_frames = 64;
     double angle0 = 0;
-    // Device copy of the analytic primitive table for the CUDA G-buffer
-    // producer (lazily created, owned here).
+    // A scene loaded from a manifest keeps its camera fixed (Camera::matrix,
+    // src/scene.rs:119-128); procedural rooms follow the orbit path.
+    bool loaded = false;
+    double cam_eye[3] = {0, 0, 0};
+    double cam_q[4] = {0, 0, 0, 1};
+    double cam_fov = 0, cam_near = 0, cam_far = 0;
+    // Device copy of the primitive table and the triangle hierarchies for
+    // the CUDA input producers (lazily created, owned here).
     void* dev_prims = nullptr;
+    void* dev_nodes = nullptr;
+    void* dev_tris = nullptr;
     int dev_prims_device = -1;
     uint32_t dev_prims_count = 0;
 
     bool build();
+    // Writes mesh m's SDF samples (res^3, x fastest) into its atlas tile at
+    // `origin`: f32 texels as they are, or f16 texels of value / scale
+    // rounded toward -inf with scale = the voxel diagonal (kept in
+    // meshes[m].lo[3]) so the dequantised field never exceeds the f32 one.
+    void store_field(uint32_t m, const float* samples, uint32_t res, const uint32_t origin[3]);
     void camera_at(uint32_t frame, double eye[3], double target[3]) const;
     M4 view_projection(uint32_t frame) const;
     void frame_data(uint32_t index, uint32_t debug, irt_frame* f, irt_object* objects, irt_node* nodes,
                     irt_light* lights) const;
     void settings(irt_settings* s) const;
+    // `cull` skips back-facing triangles (primary rays of the raster);
+    // analytic parts only report front entries either way.
     bool intersect_object(uint32_t oi, const double o[3], const double d[3], double tmin, double tmax, double& t,
-                          double n[3]) const;
+                          double n[3], bool cull = false) const;
     bool cast(const double o[3], const double d[3], double tmin, double tmax, double& t, double n[3],
-              uint32_t& object) const;
+              uint32_t& object, bool cull = false) const;
 };
 
 uint16_t f16_bits_rne(float f);
@@ -65,14 +86,24 @@ uint32_t oct_encode_snorm16(float x, float y, float z);
 // rgba8 unorm packing with round-to-nearest.
 uint32_t pack_unorm8x4(float r, float g, float b, float a);
 
-// Flattened primitive record used by the CUDA G-buffer producer.
+// Flattened primitive record used by the CUDA input producers.
+enum : uint32_t { kPrimBox = 0, kPrimSphere = 1, kPrimTriangles = 2 };
 struct GPrim {
     float inv_model[16];
     float model[16];
-    float lo[4], hi[4];  // box bounds (local) or radius in lo[0] for spheres
+    float lo[4], hi[4];  // box bounds or the triangle mesh's bounds (local); radius in lo[0] for spheres
     float color[4];
     float params[4];     // roughness, metal after material clamping
-    uint32_t object, sphere, pad0, pad1;
+    uint32_t object, kind;
+    uint32_t node_base, tri_base;  // kPrimTriangles: the mesh's hierarchy in the shared tables
+};
+
+// The primitive table and the shared triangle tables on one device.
+struct PrimTable {
+    const GPrim* prims;
+    uint32_t n;
+    const TriNode* nodes;
+    const TriRec* tris;
 };
 
 }  // namespace irt

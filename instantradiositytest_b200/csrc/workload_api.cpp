@@ -241,7 +241,7 @@ irt_status irt_workload_gbuffer_cpu(const irt_workload* wl, const irt_frame* f, 
             double t, n[3];
             uint32_t obj = 0;
             float dep = 1.f, nrm[3] = {0, 0, 0}, col[3] = {0, 0, 0}, par[2] = {0, 0}, mot[2] = {0, 0};
-            bool hit = w.cast(o, d, 0.0, 1.0, t, n, obj);
+            bool hit = w.cast(o, d, 0.0, 1.0, t, n, obj, true);
             if (hit) {
                 double p[3] = {o[0] + d[0] * t, o[1] + d[1] * t, o[2] + d[2] * t};
                 double c[4], pc[4];

@@ -24,16 +24,50 @@ def preset_spec(which: int, **overrides) -> L.WorkloadSpec:
     return spec
 
 
+class SceneLoadError(ValueError):
+    """A scene file that Scene::load / Scene::validate (src/scene.rs:157-382)
+    rejects; the message carries the reference's error context."""
+
+
 class Workload:
-    def __init__(self, spec: L.WorkloadSpec | int = 0, **overrides):
+    def __init__(self, spec: L.WorkloadSpec | int = 0, _handle=None, **overrides):
         if isinstance(spec, int):
             spec = preset_spec(spec, **overrides)
         else:
             for k, v in overrides.items():
                 setattr(spec, k, v)
         self.spec = spec
+        if _handle is None:
+            h = C.c_void_p()
+            L.check(lib.irt_workload_create(C.byref(spec), C.byref(h)), what="workload create")
+        else:
+            h = _handle
+        self._init_from_handle(h)
+
+    @classmethod
+    def load(cls, manifest_path, width: int = 1920, height: int = 1080, vpl_count: int = 1024,
+             vpl_bounces: int = 3, sdf_format: int = L.SDF_F32) -> "Workload":
+        """Scene::load (src/scene.rs:180-255) of a version-1 scene manifest and
+        its binaries: the returned workload renders the file's scene from its
+        fixed camera at width x height.  Raises SceneLoadError with the
+        reference's error text when the file is rejected."""
+        spec = L.WorkloadSpec()
+        spec.width, spec.height = width, height
+        spec.vpl_count, spec.vpl_bounces = vpl_count, vpl_bounces
+        spec.sdf_format = sdf_format
         h = C.c_void_p()
-        L.check(lib.irt_workload_create(C.byref(spec), C.byref(h)), what="workload create")
+        msg = C.create_string_buffer(1024)
+        st = lib.irt_workload_load(str(manifest_path).encode(), C.byref(spec), C.byref(h), msg, len(msg))
+        if st != L.IRT_OK:
+            if st == L.IRT_E_NOMEM:
+                raise MemoryError(msg.value.decode(errors="replace"))
+            raise SceneLoadError(msg.value.decode(errors="replace"))
+        wl = cls(spec, _handle=h)
+        wl.path = str(manifest_path)
+        return wl
+
+    def _init_from_handle(self, h):
+        spec = self.spec
         self.handle = h
         self.width, self.height = spec.width, spec.height
         self.object_count = lib.irt_workload_object_count(h)
