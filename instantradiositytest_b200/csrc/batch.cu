@@ -146,6 +146,7 @@ LightingLaunch lighting_launch(irt_session* s, const irt_scene* sc, const irt_fr
     L.lights = sc->lights_prep;
     L.atlas = sc->atlas;
     L.sdf_f16 = sc->sdf_f16;
+    L.sdf_cells = sc->sdf_cells;
     L.error = s->error;
     L.cur_vpls = cur;
     L.prev_vpls = prev;
@@ -295,6 +296,7 @@ irt_status build_tables(irt_batch* b, int p, irt_scene* const* scenes, const irt
             G.nodes = sc->nodes;
             G.atlas = sc->atlas;
             G.sdf_f16 = sc->sdf_f16;
+            G.sdf_cells = sc->sdf_cells;
             G.march_scene = sc->march_scene;
             const uint32_t bytes = irt_march_scene_bytes(sc->object_count);
             G.scene_vec4 = bytes / 16;

@@ -113,6 +113,38 @@ irt_status irt_scene_create(irt_context* ctx, const irt_mesh* meshes, uint32_t m
     td.normalizedCoords = 0;
     e = cudaCreateTextureObject(&sc->atlas, &rd, &td, nullptr);
     if (e != cudaSuccess) return fail(cuda_fail(ctx, e, "texture object"));
+    // Corner cells of the field meshes (DevScene::sdf_cells); a mesh's first
+    // record index goes into hi[3] of its rows, which nothing else reads.
+    {
+        uint64_t total = 0;
+        std::vector<uint64_t> base(mesh_count, 0);
+        for (uint32_t m = 0; m < mesh_count; m++) {
+            if (meshes[m].geometry_lo[3] > .5f) continue;
+            const uint64_t n = meshes[m].field[3] - 1u;
+            base[m] = total;
+            total += n * n * n;
+        }
+        if (total > 0xffffffffull) {
+            ctx->set_error("field meshes exceed 2^32 SDF cells");
+            return fail(IRT_E_INVALID);
+        }
+        if (total > 0) {
+            st = dev_alloc(ctx, &sc->sdf_cells, total * (sc->sdf_f16 ? 16 : 32), sc->bytes);
+            if (st) return fail(st);
+            for (uint32_t m = 0; m < mesh_count; m++) {
+                if (meshes[m].geometry_lo[3] > .5f) continue;
+                e = irt_pack_sdf_cells(sc->atlas, sc->sdf_f16, meshes[m].field, meshes[m].field[3], base[m],
+                                       sc->sdf_cells, nullptr);
+                if (e != cudaSuccess) return fail(cuda_fail(ctx, e, "corner cells"));
+                const uint32_t b32 = (uint32_t)base[m];
+                std::memcpy(&sc->host_meshes[m].hi[3], &b32, 4);
+            }
+            e = cudaStreamSynchronize(nullptr);
+            if (e != cudaSuccess) return fail(cuda_fail(ctx, e, "corner cells"));
+            e = cudaMemcpy(sc->meshes, sc->host_meshes.data(), sizeof(irt_mesh) * mesh_count, cudaMemcpyHostToDevice);
+            if (e != cudaSuccess) return fail(cuda_fail(ctx, e, "mesh upload"));
+        }
+    }
     ctx->in_use += sc->bytes;
     *out = sc;
     return IRT_OK;
@@ -280,6 +312,7 @@ irt_status irt_scene_update(irt_scene* sc, const irt_object* objects, uint32_t o
         LC.n = object_count;
         LC.atlas = sc->atlas;
         LC.sdf_f16 = sc->sdf_f16;
+        LC.sdf_cells = sc->sdf_cells;
         for (int a = 0; a < 3; a++) {
             // The grid covers the root box grown by 0.1 % and 1 mm.
             double ext = (double)nodes[0].hi[a] - (double)nodes[0].lo[a];
@@ -327,6 +360,7 @@ void irt_scene_destroy(irt_scene* sc) {
     DeviceGuard g(sc->ctx->device);
     if (sc->atlas) cudaDestroyTextureObject(sc->atlas);
     if (sc->atlas_array) cudaFreeArray(sc->atlas_array);
+    if (sc->sdf_cells) cudaFree(sc->sdf_cells);
     if (sc->meshes) cudaFree(sc->meshes);
     if (sc->objects) cudaFree(sc->objects);
     if (sc->nodes) cudaFree(sc->nodes);
@@ -562,6 +596,7 @@ irt_status irt_frame_lighting(irt_session* s, const irt_scene* sc, const irt_fra
     L.lights = sc->lights_prep;
     L.atlas = sc->atlas;
     L.sdf_f16 = sc->sdf_f16;
+    L.sdf_cells = sc->sdf_cells;
     L.error = s->error;
     L.cur_vpls = cur;
     L.prev_vpls = prev;
@@ -597,6 +632,7 @@ irt_status irt_frame_lighting(irt_session* s, const irt_scene* sc, const irt_fra
         M.nodes = sc->nodes;
         M.atlas = sc->atlas;
         M.sdf_f16 = sc->sdf_f16;
+        M.sdf_cells = sc->sdf_cells;
         M.error = s->error;
         M.march_scene = sc->march_scene;
         M.cells = sc->cells;

@@ -34,6 +34,10 @@ struct irt_scene {
     cudaTextureObject_t atlas = 0;
     int sdf_f16 = 0;
     uint32_t atlas_dims[3] = {0, 0, 0};
+    // Corner cells: per field mesh, the 8 corner texels of each of its
+    // (res-1)^3 cells in one record (f32: 32 B, f16: 16 B); a mesh's first
+    // cell index is in hi[3] of its rows (host_meshes and the device copy).
+    void* sdf_cells = nullptr;
     std::vector<irt_mesh> host_meshes;
     // per-frame data
     irt_object* objects = nullptr;

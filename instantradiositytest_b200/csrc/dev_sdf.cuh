@@ -15,6 +15,12 @@ struct DevScene {
     cudaTextureObject_t atlas;  // 3-D R32F or R16F texels, point sampled
     int32_t sdf_f16;            // texel = f16(value / mesh.lo[3])
     uint32_t* error;            // device error word
+    // Corner cells of the field meshes, built from the atlas at scene
+    // creation (sdfcells.cu): cell (cx, cy, cz) of a mesh of resolution res
+    // is record bits(mesh.hi[3]) + (cz * (res-1) + cy) * (res-1) + cx,
+    // holding the 8 texels t[k] at (cx + (k&1), cy + (k>>1 & 1), cz + (k>>2))
+    // of its atlas tile — two float4 (f32) or eight halves in one uint4 (f16).
+    const void* sdf_cells;
 };
 
 // Read-only-path loads of the scene records as 16-byte vectors.
@@ -64,7 +70,7 @@ __device__ __forceinline__ float signed_box_distance(V3 p, V3 lo, V3 hi) {
     return length(vmax(delta, V3{0.f, 0.f, 0.f})) + wmin(wmax(delta.x, wmax(delta.y, delta.z)), 0.f);
 }
 
-// common.wgsl:31-38 — 8 texel loads, cell clamped to res-2, weights in
+// common.wgsl:31-38 — the 8 texels of the cell (clamped to res-2), weights in
 // z, y, x order as the WGSL loop accumulates them.
 __device__ __forceinline__ float sample_field(const DevScene& sc, const DMesh& m, V3 q) {
     uint32_t res = m.field.w;
@@ -72,13 +78,25 @@ __device__ __forceinline__ float sample_field(const DevScene& sc, const DMesh& m
     uint32_t cy = min(to_u32(floorf(q.y)), res - 2u);
     uint32_t cz = min(to_u32(floorf(q.z)), res - 2u);
     float fx = q.x - (float)cx, fy = q.y - (float)cy, fz = q.z - (float)cz;
-    float bx = (float)(m.field.x + cx) + 0.5f;
-    float by = (float)(m.field.y + cy) + 0.5f;
-    float bz = (float)(m.field.z + cz) + 0.5f;
+    // One 32-byte (f32) or 16-byte (f16) corner record per cell instead of 8
+    // texture fetches; the same texel values.
     float t[8];
+    const uint32_t n = res - 1u;
+    const uint32_t cell = __float_as_uint(m.hi.w) + (cz * n + cy) * n + cx;
+    if (sc.sdf_f16) {
+        const uint4 h = __ldg(static_cast<const uint4*>(sc.sdf_cells) + cell);
+        const uint32_t w[4] = {h.x, h.y, h.z, h.w};
 #pragma unroll
-    for (int k = 0; k < 8; k++)
-        t[k] = tex3D<float>(sc.atlas, bx + (float)(k & 1), by + (float)((k >> 1) & 1), bz + (float)(k >> 2));
+        for (int k = 0; k < 4; k++) {
+            t[2 * k] = __half2float(__ushort_as_half((unsigned short)(w[k] & 0xffffu)));
+            t[2 * k + 1] = __half2float(__ushort_as_half((unsigned short)(w[k] >> 16)));
+        }
+    } else {
+        const float4* c = static_cast<const float4*>(sc.sdf_cells) + 2 * (size_t)cell;
+        const float4 a = __ldg(c), b = __ldg(c + 1);
+        t[0] = a.x, t[1] = a.y, t[2] = a.z, t[3] = a.w;
+        t[4] = b.x, t[5] = b.y, t[6] = b.z, t[7] = b.w;
+    }
     if (sc.sdf_f16) {
         float s = m.lo.w;
 #pragma unroll

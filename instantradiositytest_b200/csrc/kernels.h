@@ -31,6 +31,7 @@ struct LightingLaunch {
     const irt_light* lights;
     cudaTextureObject_t atlas;
     int sdf_f16;
+    const void* sdf_cells;  // corner cells of the field meshes (dev_sdf.cuh), or null
     uint32_t* error;
     const irt_vpl* cur_vpls;
     const irt_vpl* prev_vpls;
@@ -59,6 +60,7 @@ struct MarchLaunch {
     const irt_node* nodes;
     cudaTextureObject_t atlas;
     int sdf_f16;
+    const void* sdf_cells;  // corner cells of the field meshes (dev_sdf.cuh), or null
     uint32_t* error;
     const float4* march_scene;  // compact nodes + objects (irt_march_scene_bytes)
     // Leaf-order cache: a kGridRes^3 grid over the root box; per cell the
@@ -88,6 +90,7 @@ struct LeafCacheLaunch {
     uint32_t n;                 // objects
     cudaTextureObject_t atlas;
     int sdf_f16;
+    const void* sdf_cells;  // corner cells of the field meshes (dev_sdf.cuh), or null
     double grid_org_d[3], grid_size_d[3];
     float* corners;             // (kGridRes+1)^3 * n floats, or null: box bounds only
     uint32_t* cells;            // kGridRes^3 * kCellWords words
@@ -133,6 +136,11 @@ cudaError_t irt_workload_prims(const irt_workload* wl, irt::PrimTable* out);
 
 cudaError_t irt_launch_lighting(const LightingLaunch& L, int stage, cudaStream_t st);
 
+// Corner cells of one field mesh (sdfcells.cu): records [base, base +
+// (res-1)^3) of `out` from the atlas tile at `origin` (DevScene::sdf_cells).
+cudaError_t irt_pack_sdf_cells(cudaTextureObject_t atlas, int f16, const uint32_t origin[3], uint32_t res,
+                               uint64_t base, void* out, cudaStream_t st);
+
 // ------------------------------------------------------------------ batched views
 // One launch per pass over the views of a batch.  `table` is a device array
 // of n per-view argument records of the stage (lighting: the LightArgs of
@@ -176,6 +184,7 @@ struct alignas(16) MarchGroup {
     const irt_node* nodes;
     cudaTextureObject_t atlas;
     int sdf_f16;
+    const void* sdf_cells;  // corner cells of the field meshes (dev_sdf.cuh), or null
     uint32_t* error;
     const float4* march_scene;
     uint32_t scene_vec4;

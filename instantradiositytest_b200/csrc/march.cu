@@ -232,6 +232,7 @@ __global__ void __launch_bounds__(128, 6) march_batched_kernel(const MarchGroup*
         sc.lights = nullptr;
         sc.atlas = G.atlas;
         sc.sdf_f16 = G.sdf_f16;
+        sc.sdf_cells = G.sdf_cells;
         sc.error = G.error;
         Grid grid;
         grid.cells = G.cells;
@@ -365,6 +366,7 @@ cudaError_t IRT_MARCH_LAUNCH(const MarchLaunch& M, cudaStream_t st) {
     sc.lights = nullptr;
     sc.atlas = M.atlas;
     sc.sdf_f16 = M.sdf_f16;
+    sc.sdf_cells = M.sdf_cells;
     sc.error = M.error;
     Grid g;
     g.cells = M.cells;

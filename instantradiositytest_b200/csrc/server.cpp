@@ -110,6 +110,8 @@ extern "C" uint64_t irt_server_request_bytes(const irt_server* s, const irt_requ
     const uint64_t atlas = (uint64_t)w.atlas_dims[0] * w.atlas_dims[1] * w.atlas_dims[2] * texel;
     uint64_t scene = atlas + atlas / 8 + (4u << 20);                 // atlas (+ array padding), leaf cache
     scene += n * (208 + 2 * 48 + 176 + 33ull * 33 * 33 * 4) + 128 * w.meshes.size() + 2 * 48 * w.lights.size();
+    for (const irt_mesh& m : w.meshes)  // corner cells of the field meshes (8 texels per cell)
+        if (m.geometry_lo[3] <= .5f) scene += (uint64_t)(m.field[3] - 1) * (m.field[3] - 1) * (m.field[3] - 1) * texel * 8;
     const uint64_t inputs = P * gbuffer_bytes_per_pixel(s->d.gbuffer_format) + 3ull * sd.settings.vpl_count * 48;
     return irt_session_bytes(&sd) + scene + inputs;
 }
