@@ -98,18 +98,29 @@ __device__ __forceinline__ void atrous_body(const irt_frame& f, const SvgfCtx<G>
     V3 sum = V3{0.f, 0.f, 0.f};
     float total = 0.f, v = 0.f;
     float lc = luminance(V3{c4.x, c4.y, c4.z});
-    for (int32_t yy = -2; yy <= 2; yy++)
-        for (int32_t xx = -2; xx <= 2; xx++) {
-            int32_t qx = x + xx * step, qy = y + yy * step;
-            float geom = sv.geometry_weight(a, qx, qy, (float)step);
-            if (geom <= 0.f) continue;
-            float4 smp = R::load(input, sv.idx(qx, qy));
-            float w = wavelet_kernel(xx) * wavelet_kernel(yy) * geom *
-                      expf(-fabsf(luminance(V3{smp.x, smp.y, smp.z}) - lc) / phi);
-            sum = sum + V3{smp.x, smp.y, smp.z} * w;
-            v += smp.w * smp.w * w * w;
-            total += w;
-        }
+    auto tap = [&](int32_t xx, int32_t yy) {
+        int32_t qx = x + xx * step, qy = y + yy * step;
+        float geom = sv.geometry_weight(a, qx, qy, (float)step);
+        if (geom <= 0.f) return;
+        float4 smp = R::load(input, sv.idx(qx, qy));
+        float w = wavelet_kernel(xx) * wavelet_kernel(yy) * geom *
+                  expf(-fabsf(luminance(V3{smp.x, smp.y, smp.z}) - lc) / phi);
+        sum = sum + V3{smp.x, smp.y, smp.z} * w;
+        v += smp.w * smp.w * w * w;
+        total += w;
+    };
+    // Taps in row order.  With feature records (three 128-bit loads a tap)
+    // a row's five taps are unrolled so their loads issue together (a-trous
+    // 1.12 -> 1.03 ms at 1920x1200); on f32 planes (six loads a tap) the
+    // unrolled row needs more registers than it saves (1.08 -> 1.23 ms).
+    if constexpr (Sv<G>::kFeatures) {
+        for (int32_t yy = -2; yy <= 2; yy++)
+#pragma unroll
+            for (int32_t xx = -2; xx <= 2; xx++) tap(xx, yy);
+    } else {
+        for (int32_t yy = -2; yy <= 2; yy++)
+            for (int32_t xx = -2; xx <= 2; xx++) tap(xx, yy);
+    }
     float dn = wmax(total, .00001f);
     float4 o = make_float4(sum.x / dn, sum.y / dn, sum.z / dn, wmin(sqrtf(v) / dn, 65000.f));
     R::store(out, i, o);
