@@ -97,6 +97,17 @@ __device__ __forceinline__ float sample_field(const DevScene& sc, const DMesh& m
         t[0] = a.x, t[1] = a.y, t[2] = a.z, t[3] = a.w;
         t[4] = b.x, t[5] = b.y, t[6] = b.z, t[7] = b.w;
     }
+#if IRT_MARCH_FAST
+    // The fast march: the same trilinear value as three lerp stages and the
+    // f16 scale applied once — 14 operations for ~40; the rounding differs
+    // from the weight sums in the last bits, as its approximate division and
+    // square root do, far inside the field bound's voxel/128 margin.
+    const float x0 = fmaf(fx, t[1] - t[0], t[0]), x1 = fmaf(fx, t[3] - t[2], t[2]);
+    const float x2 = fmaf(fx, t[5] - t[4], t[4]), x3 = fmaf(fx, t[7] - t[6], t[6]);
+    const float y0 = fmaf(fy, x1 - x0, x0), y1 = fmaf(fy, x3 - x2, x2);
+    const float value = fmaf(fz, y1 - y0, y0);
+    return sc.sdf_f16 ? value * m.lo.w : value;
+#else
     if (sc.sdf_f16) {
         float s = m.lo.w;
 #pragma unroll
@@ -111,6 +122,7 @@ __device__ __forceinline__ float sample_field(const DevScene& sc, const DMesh& m
         value += t[k] * wx * wy * wz;
     }
     return value;
+#endif
 }
 
 // sdf.wgsl:5-33
