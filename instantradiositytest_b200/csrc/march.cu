@@ -207,10 +207,12 @@ __global__ void __launch_bounds__(128, 8) march_kernel(const __grid_constant__ i
 // Batched march: for each scene group the CTA stages the group record and
 // its compact scene in shared memory, then its warps consume the group's ray
 // queues (one per view) in order with the same per-lane state machine; a
-// lane keeps the visibility array of the queue its ray came from.
+// lane keeps the address of its ray record and the index of the queue it
+// came from, and re-reads the record's target, endpoint normal and output
+// slot where a phase needs them (as march_kernel does).
 constexpr uint32_t kGroupVec4 = (uint32_t)((sizeof(MarchGroup) + 15) / 16);
 
-__global__ void __launch_bounds__(128, 6) march_batched_kernel(const MarchGroup* __restrict__ groups, uint32_t n_groups,
+__global__ void __launch_bounds__(128, 8) march_batched_kernel(const MarchGroup* __restrict__ groups, uint32_t n_groups,
                                                             const MarchQueue* __restrict__ queues) {
     extern __shared__ float4 smem[];
     const MarchGroup& G = *reinterpret_cast<const MarchGroup*>(smem);
@@ -252,8 +254,8 @@ __global__ void __launch_bounds__(128, 6) march_batched_kernel(const MarchGroup*
         bool exhausted = q >= G.q_end;
         uint32_t n_rays = exhausted ? 0u : *(volatile const uint32_t*)&queues[q].counters[0];
         bool active = false;
-        uint32_t phase = kClear, slot = 0;
-        float* vis = nullptr;
+        uint32_t phase = kClear, lq = 0;
+        const float4* rec = nullptr;
         MarchState m;
         m.closest = kNone;
         m.origin = V3{0.f, 0.f, 0.f};
@@ -262,7 +264,6 @@ __global__ void __launch_bounds__(128, 6) march_batched_kernel(const MarchGroup*
         m.result = 1.f;
         m.previous = 1e20f;
         m.step = 0;
-        V3 target{0.f, 0.f, 0.f}, endn{0.f, 0.f, 0.f};
         for (;;) {
             if (!exhausted) {
                 unsigned need = __ballot_sync(full, !active);
@@ -276,15 +277,12 @@ __global__ void __launch_bounds__(128, 6) march_batched_kernel(const MarchGroup*
                     if (!active) {
                         uint32_t idx = base + (uint32_t)__popc(need & ((1u << lane) - 1u));
                         if (idx < n_rays) {
-                            const float4* r = reinterpret_cast<const float4*>(Q.rays + idx);
-                            float4 a = __ldg(r), b = __ldg(r + 1), c = __ldg(r + 2), d = __ldg(r + 3);
+                            rec = reinterpret_cast<const float4*>(Q.rays + idx);
+                            float4 a = __ldg(rec), b = __ldg(rec + 1);
                             m.origin = V3{a.x, a.y, a.z};
-                            slot = __float_as_uint(a.w);
                             m.dir = V3{b.x, b.y, b.z};
-                            target = V3{c.x, c.y, c.z};
-                            endn = V3{d.x, d.y, d.z};
                             phase = kClear;
-                            vis = Q.vis;
+                            lq = q;
                             active = true;
                         }
                     }
@@ -301,7 +299,7 @@ __global__ void __launch_bounds__(128, 6) march_batched_kernel(const MarchGroup*
             }
             if (!active) continue;
 
-            V3 qp = phase == kClear ? m.origin : (phase == kEndpoint ? target : march_point(m));
+            V3 qp = phase == kClear ? m.origin : (phase == kEndpoint ? xyz(__ldg(rec + 2)) : march_point(m));
             uint32_t hint = phase == kMarch ? m.closest : kNone;
             Dist d = scene_distance_cached(sc, f, grid, nodes, objs, qp, hint, phase != kMarch);
 
@@ -309,21 +307,24 @@ __global__ void __launch_bounds__(128, 6) march_batched_kernel(const MarchGroup*
             if (phase == kClear) {
                 m.closest = d.closest;
                 m.origin = m.origin + m.dir * clearance_epsilon(eps, d.voxel);
+                const V3 endn = xyz(__ldg(rec + 3));
                 if (dot(endn, endn) > .5f) {
                     phase = kEndpoint;
                 } else {
                     phase = kMarch;
-                    out = march_begin(m, target, eps, max_steps);
+                    out = march_begin(m, xyz(__ldg(rec + 2)), eps, max_steps);
                 }
             } else if (phase == kEndpoint) {
                 phase = kMarch;
+                const V3 target = xyz(__ldg(rec + 2)), endn = xyz(__ldg(rec + 3));
                 out = march_begin(m, target + endn * clearance_epsilon(eps, d.voxel), eps, max_steps);
             } else {
                 m.closest = d.closest;
                 out = march_after(m, d.best, eps, f.sdf[2], max_steps);
             }
             if (out >= 0.f) {
-                vis[slot] = out;
+                float* vis = queues[lq].vis;
+                vis[__float_as_uint(__ldg(rec).w)] = out;
                 active = false;
             }
         }
