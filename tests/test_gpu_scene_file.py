@@ -76,9 +76,9 @@ def producers_agree(path, width, height, vpls):
     ctx.close()
 
 
-def lockstep(path, width, height, vpls, frames):
-    wl = Workload.load(path, width=width, height=height, vpl_count=vpls)
-    ls = Lockstep(wl)
+def lockstep(path, width, height, vpls, frames, sdf_format=L.SDF_F32, **formats):
+    wl = Workload.load(path, width=width, height=height, vpl_count=vpls, sdf_format=sdf_format)
+    ls = Lockstep(wl, **formats)
     rows = [ls.frame(i) for i in range(frames)]
     ls.close()
     worst = {k: (min(r[k] for r in rows) if k.startswith("select") else max(r[k] for r in rows)) for k in rows[0]}
@@ -96,6 +96,47 @@ def test_cuda_producers_match_cpu_on_a_loaded_scene(cuda, demo):
 
 def test_loaded_scene_lockstep_parity(cuda, demo):
     lockstep(demo, 192, 120, 256, 8)
+
+
+def test_loaded_scene_mixed_precision_lockstep(cuda, demo):
+    """The loaded scene with the mixed-precision storage: f16 SDF corner
+    records, packed G-buffer, f16 radiance and moments; the oracle sees the
+    same quantised inputs and the reference's f16 storage points."""
+    lockstep(demo, 192, 120, 256, 6, sdf_format=L.SDF_F16, gbuffer_format=L.GBUFFER_PACKED,
+             radiance_format=L.RADIANCE_F16, moments_format=L.MOMENTS_F16)
+
+
+def test_batched_views_of_a_loaded_scene_equal_alone(cuda, demo):
+    """A batch over a loaded scene and a procedural room (views of uneven
+    size, two views of the loaded scene): every view's outputs equal
+    rendering it alone, bit for bit."""
+    from instantradiositytest_b200.batching import BatchDriver
+    from test_gpu_batch import BUFS, render_alone, workload
+
+    a = Workload.load(demo, width=160, height=100, vpl_count=128)
+    b = workload(31, 10, 128, 80)
+    views = [(a, 0), (b, 0), (a, 5, (96, 60))]
+    ctx = Context()
+    drv = BatchDriver(ctx, views, use_graphs=True)
+    per_view = [[] for _ in views]
+    for i in range(8):
+        data = drv.inputs(i)
+        frames = drv.step(i, data)
+        for v, (f, (_, obj, nodes, lights)) in enumerate(zip(frames, data)):
+            per_view[v].append((L.Frame.from_buffer_copy(f), obj, nodes, lights))
+    torch.cuda.synchronize()
+    for v, view in enumerate(views):
+        wl = view[0]
+        if len(view) > 2:  # the alone render runs at the view's own size
+            continue
+        s = drv.batch.view(v)
+        got = {w: s.buffer(w, torch.uint8).cpu().numpy() for w in BUFS}
+        ref = render_alone(ctx, wl, per_view[v], L.GBUFFER_F32, L.RADIANCE_F32, L.MOMENTS_F32)
+        for w in BUFS:
+            assert np.array_equal(got[w], ref[w]), (v, w)
+    assert np.isfinite(drv.batch.view(2).image_host(L.BUF_FILTERED)).all()
+    drv.close()
+    ctx.close()
 
 
 @pytest.mark.skipif(not (SHIPPED and os.path.exists(SHIPPED)), reason="IRT_TEST_SCENE not set")
