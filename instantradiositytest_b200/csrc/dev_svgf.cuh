@@ -96,15 +96,18 @@ struct Sv {
         return world(uvx(x), uvy(y), c.g.d(idx(x, y)), f.inv_vp);
     }
     // svgf.wgsl:20-26
-    __device__ __forceinline__ bool history_ok(int32_t px, int32_t py, int32_t qx, int32_t qy) const {
+    // `a`, `n`: the pixel's position and (decoded) normal, `reach` =
+    // temporal[1] * max(distance(a, camera), 1) — the same for its 4 taps.
+    __device__ __forceinline__ bool history_ok(V3 a, V3 n, float reach, int32_t qx, int32_t qy) const {
         if (f.flags[0] == 0u || f.flags[1] != f.size[3] || !inside(qx, qy)) return false;
         size_t q = idx(qx, qy);
         float d = __ldg(c.old_depth + q);
         if (d >= 1.f) return false;
-        V3 a = position(px, py);
         V3 b = c.old_guide ? xyz(__ldg(c.old_guide + q)) : world(uvx(qx), uvy(qy), d, f.previous_inv_vp);
-        return distance(a, b) < f.temporal[1] * wmax(distance(a, camera()), 1.f) &&
-               dot(c.g.n(idx(px, py)), G::decode_normal(__ldg(c.old_normal + q))) > f.temporal[2];
+        return distance(a, b) < reach && dot(n, G::decode_normal(__ldg(c.old_normal + q))) > f.temporal[2];
+    }
+    __device__ __forceinline__ float history_reach(V3 a) const {
+        return f.temporal[1] * wmax(distance(a, camera()), 1.f);
     }
     // svgf.wgsl:28-31
     __device__ __forceinline__ Guide guide(int32_t x, int32_t y) const {

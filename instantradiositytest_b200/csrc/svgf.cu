@@ -38,12 +38,15 @@ __device__ __forceinline__ void temporal_body(const irt_frame& f, const SvgfCtx<
         float flx = floorf(px), fly = floorf(py);
         int32_t bx = to_i32(flx), by = to_i32(fly);
         float fx = px - flx, fy = py - fly;
+        // The pixel's own terms of the 4 history tests, computed once.
+        const V3 pa = sv.position(x, y), pn = c.g.n(i);
+        const float reach = sv.history_reach(pa);
 #pragma unroll
         for (int32_t yy = 0; yy < 2; yy++)
 #pragma unroll
             for (int32_t xx = 0; xx < 2; xx++) {
                 int32_t qx = bx + xx, qy = by + yy;
-                if (!sv.history_ok(x, y, qx, qy)) continue;
+                if (!sv.history_ok(pa, pn, reach, qx, qy)) continue;
                 size_t q = sv.idx(qx, qy);
                 Moments m = M::load(old_moments, q);
                 if (m.age <= 0.f) continue;
