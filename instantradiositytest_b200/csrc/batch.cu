@@ -167,6 +167,7 @@ LightingLaunch lighting_launch(irt_session* s, const irt_scene* sc, const irt_fr
     L.pending = s->pending;
     L.guide = s->guide[0];
     L.old_guide = s->guide[1];
+    L.feat = s->desc.gbuffer_format == IRT_GBUFFER_F32 ? nullptr : s->feat;
     return L;
 }
 

@@ -617,6 +617,7 @@ irt_status irt_frame_lighting(irt_session* s, const irt_scene* sc, const irt_fra
     L.pending = s->pending;
     L.guide = s->guide[0];
     L.old_guide = s->guide[1];
+    L.feat = s->desc.gbuffer_format == IRT_GBUFFER_F32 ? nullptr : s->feat;
     if (s->desc.fused == 1) {
         // candidates+temporal -> spatial + resolve set-up (ray queue) ->
         // persistent march -> resolve outputs.

@@ -46,6 +46,7 @@ struct LightingLaunch {
     int keep_candidates;
     const float4* guide;      // world positions of this frame's pixels
     const float4* old_guide;  // ... of the previous frame's pixels
+    const float4* feat;       // decoded normal/colour/params of this frame's pixels (f16, packed), or null
     // ray-queue resolve (kStageSpatial / march / kStageCombine)
     RayRecord* rays;         // capacity 2 * W * H
     uint32_t* ray_counters;  // [0] rays emitted, [1] rays fetched by the march

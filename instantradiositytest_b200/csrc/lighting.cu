@@ -13,6 +13,8 @@
 // row, so every own-pixel access is a coalesced 128-bit vector access).
 #include <cuda_runtime.h>
 
+#include <type_traits>
+
 #include "dev_sdf.cuh"
 #include "kernels.h"
 
@@ -37,6 +39,7 @@ struct LightArgs {
     float4* pending;
     const float4* guide;      // world positions of this frame's pixels
     const float4* old_guide;  // ... of the previous frame's pixels
+    const float4* feat;       // decoded (normal, rough), (colour, metal) per pixel, or null
 };
 
 template <class G>
@@ -55,9 +58,28 @@ struct Px {
     // lighting.wgsl:30-34
     // world(pixel_uv(p), depth, inv_vp) of pixel i, precomputed per frame.
     __device__ __forceinline__ V3 position(size_t i) const { return xyz(__ldg(a.guide + i)); }
+    // Normal of pixel i as the G-buffer stores it: for the f16 and packed
+    // formats from the frame's decoded feature records (the same values the
+    // decode gives), else from the f32 plane.
+    __device__ __forceinline__ V3 normal_of(size_t i) const {
+        if constexpr (!std::is_same<G, GbF32>::value)
+            if (a.feat) return xyz(__ldg(a.feat + 2 * i));
+        return a.g.n(i);
+    }
     __device__ __forceinline__ Surface surface() const {
         Surface s;
         s.p = position(id);
+        if constexpr (!std::is_same<G, GbF32>::value) {
+            if (a.feat) {
+                const float4 n = __ldg(a.feat + 2 * id), k = __ldg(a.feat + 2 * id + 1);
+                s.n = normalize(xyz(n));
+                s.color = xyz(k);
+                s.rough = n.w;
+                s.metal = k.w;
+                surface_terms(s, camera());
+                return s;
+            }
+        }
         s.n = normalize(a.g.n(id));
         s.color = a.g.c(id);
         float2 rm = a.g.pm(id);
@@ -72,7 +94,7 @@ struct Px {
         float d = a.g.d(q);
         if (d >= 1.f) return false;
         V3 p = position(q);
-        V3 n = normalize(a.g.n(q));
+        V3 n = normalize(normal_of(q));
         return dot(s.n, n) > f.temporal[2] && distance(s.p, p) < f.temporal[1] * wmax(distance(s.p, camera()), 1.f);
     }
     // lighting.wgsl:41-44
@@ -593,6 +615,7 @@ static LightArgs<G> make_args(const LightingLaunch& L) {
     a.pending = L.pending;
     a.guide = L.guide;
     a.old_guide = L.old_guide;
+    a.feat = L.feat;
     return a;
 }
 
