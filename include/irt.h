@@ -388,7 +388,8 @@ void irt_workload_settings(const irt_workload* wl, irt_settings* out);
  * Renderer::encode (src/renderer.rs:1687-1782).  `debug` is the debug mode. */
 irt_status irt_workload_frame(irt_workload* wl, uint32_t index, uint32_t debug, irt_frame* frame,
                               irt_object* objects, irt_node* nodes, irt_light* lights);
-/* CPU G-buffer producer (analytic primary rays), writing the host planes of
+/* CPU G-buffer producer (primary rays against the workload's analytic solids
+ * or triangle hierarchies, back faces culled), writing the host planes of
  * `format` (see IRT_GBUFFER_*): depth, normal, color, params, motion. */
 irt_status irt_workload_gbuffer_cpu(const irt_workload* wl, const irt_frame* frame,
                                     const irt_object* objects, int32_t format, float* depth,
