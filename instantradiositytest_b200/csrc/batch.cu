@@ -288,7 +288,7 @@ irt_status build_tables(irt_batch* b, int p, irt_scene* const* scenes, const irt
                 if (scenes[v] != sc) continue;
                 if (queues.size() == G.q_begin) G.f = frames[v];
                 irt_session* s = b->sess[v];
-                queues.push_back(MarchQueue{s->rays, s->ray_counters, s->vis});
+                queues.push_back(MarchQueue{s->rays, s->ray_counters, s->vis, (uint32_t)(2 * s->P)});
                 if (!G.error) G.error = s->error;
             }
             G.q_end = (uint32_t)queues.size();

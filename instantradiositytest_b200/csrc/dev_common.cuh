@@ -14,6 +14,14 @@
 
 namespace irtd {
 
+// The ray queue of the march holds 2*W*H records: one class of shadow rays
+// fills it from the front (counter [0]), the other from the back (counter
+// [2]); the march takes the [0] + [2] rays in queue order, queue position i
+// being record slot ray_slot(i).
+__device__ __forceinline__ uint32_t ray_slot(uint32_t i, uint32_t front, uint32_t cap) {
+    return i < front ? i : cap - 1u - (i - front);
+}
+
 // ------------------------------------------------------------------ float3
 struct V3 {
     float x, y, z;

@@ -49,7 +49,7 @@ struct LightingLaunch {
     const float4* feat;       // decoded normal/colour/params of this frame's pixels (f16, packed), or null
     // ray-queue resolve (kStageSpatial / march / kStageCombine)
     RayRecord* rays;         // capacity 2 * W * H
-    uint32_t* ray_counters;  // [0] rays emitted, [1] rays fetched by the march
+    uint32_t* ray_counters;  // [0] VPL rays (queue front), [1] rays fetched by the march, [2] light rays (back)
     float* vis;              // visibility per pixel * 2 + kind
     float4* pending;         // per pixel: direct contribution (w = 1: x vis), indirect (w = 1: x vis)
 };
@@ -175,8 +175,9 @@ cudaError_t irt_launch_svgf_spatial_batched(const BatchLaunch& B, int stage, cud
 // view) are consumed in order.
 struct MarchQueue {
     const RayRecord* rays;
-    uint32_t* counters;
+    uint32_t* counters;  // [0] rays at the front, [1] rays fetched, [2] rays at the back
     float* vis;
+    uint32_t cap;        // records (2 * W * H)
 };
 struct alignas(16) MarchGroup {
     irt_frame f;                // counts[3] and sdf[] of the group's views

@@ -339,6 +339,9 @@ __global__ void __launch_bounds__(256) shade_kernel(const __grid_constant__ irt_
 // clearance query); each ray's result slot is in its record, so the order
 // changes no result.  The records' fields stay in registers (no indexed
 // local array).
+// Queue ends of the two ray classes: counter 0 fills from the front, 2 from the back.
+constexpr uint32_t kVplCounter = 0, kLightCounter = 2;
+
 template <class G, class R>
 __device__ __forceinline__ void spatial_prep_body(const irt_frame& f, const LightArgs<G>& a, uint32_t x, uint32_t y) {
     const bool in = x < f.size[0] && y < f.size[1];
@@ -401,20 +404,29 @@ __device__ __forceinline__ void spatial_prep_body(const irt_frame& f, const Ligh
     // lane within the warp for any 2-D block shape (warps take consecutive linear thread ids)
     const uint32_t lane = (threadIdx.y * blockDim.x + threadIdx.x) & 31u;
     const unsigned bd = __ballot_sync(full, ray_d), bi = __ballot_sync(full, ray_i);
-    const uint32_t nd = (uint32_t)__popc(bd), total = nd + (uint32_t)__popc(bi);
-    uint32_t base = 0;
-    if (lane == 0 && total > 0) base = atomicAdd(a.ray_counters, total);
-    base = __shfl_sync(full, base, 0);
+    const uint32_t nd = (uint32_t)__popc(bd), ni = (uint32_t)__popc(bi);
+    // VPL rays from the front of the queue, light rays from the back
+    // (ray_slot), so the march takes all VPL rays, then all light rays.
+    uint32_t base_i = 0, base_d = 0;
+    if (lane == 0) {
+        if (ni) base_i = atomicAdd(a.ray_counters + kVplCounter, ni);
+        if (nd) base_d = atomicAdd(a.ray_counters + kLightCounter, nd);
+    }
+    base_i = __shfl_sync(full, base_i, 0);
+    base_d = __shfl_sync(full, base_d, 0);
+    const uint32_t cap = 2u * f.size[0] * f.size[1];
     const unsigned below = (1u << lane) - 1u;
     if (ray_d) {
-        float4* r = reinterpret_cast<float4*>(a.rays + base + (uint32_t)__popc(bd & below));
+        const uint32_t k = base_d + (uint32_t)__popc(bd & below);
+        float4* r = reinterpret_cast<float4*>(a.rays + (kLightCounter == 0 ? k : cap - 1u - k));
         r[0] = make_float4(sp.x, sp.y, sp.z, __uint_as_float((uint32_t)(id * 2)));
         r[1] = make_float4(sn.x, sn.y, sn.z, 0.f);
         r[2] = make_float4(lpos.x, lpos.y, lpos.z, 0.f);
         r[3] = make_float4(0.f, 0.f, 0.f, 0.f);
     }
     if (ray_i) {
-        float4* r = reinterpret_cast<float4*>(a.rays + base + nd + (uint32_t)__popc(bi & below));
+        const uint32_t k = base_i + (uint32_t)__popc(bi & below);
+        float4* r = reinterpret_cast<float4*>(a.rays + (kVplCounter == 0 ? k : cap - 1u - k));
         r[0] = make_float4(sp.x, sp.y, sp.z, __uint_as_float((uint32_t)(id * 2 + 1)));
         r[1] = make_float4(sn.x, sn.y, sn.z, 1.f);
         r[2] = make_float4(vpos.x, vpos.y, vpos.z, 0.f);

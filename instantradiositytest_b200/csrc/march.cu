@@ -126,7 +126,9 @@ __global__ void __launch_bounds__(128, 8) march_kernel(const __grid_constant__ i
     const MNode* nodes = reinterpret_cast<const MNode*>(smem);
     const MObj* objs = reinterpret_cast<const MObj*>(smem + 2 * (2 * n_obj - 1));
 
-    const uint32_t n_rays = *(volatile uint32_t*)&counters[0];
+    const uint32_t front = *(volatile uint32_t*)&counters[0];
+    const uint32_t n_rays = front + *(volatile uint32_t*)&counters[2];
+    const uint32_t cap = 2u * f.size[0] * f.size[1];
     const unsigned full = 0xffffffffu;
     const int lane = threadIdx.x & 31;
     const float eps = f.sdf[1];
@@ -159,11 +161,11 @@ __global__ void __launch_bounds__(128, 8) march_kernel(const __grid_constant__ i
                 if (!active) {
                     uint32_t idx = base + (uint32_t)__popc(need & ((1u << lane) - 1u));
                     if (idx < n_rays) {
-                        const float4* r = reinterpret_cast<const float4*>(rays + idx);
+                        ridx = ray_slot(idx, front, cap);
+                        const float4* r = reinterpret_cast<const float4*>(rays + ridx);
                         float4 a = __ldg(r), b = __ldg(r + 1);
                         m.origin = V3{a.x, a.y, a.z};
                         m.dir = V3{b.x, b.y, b.z};
-                        ridx = idx;
                         phase = kClear;
                         active = true;
                     }
@@ -252,7 +254,8 @@ __global__ void __launch_bounds__(128, 8) march_batched_kernel(const MarchGroup*
 
         uint32_t q = G.q_begin;
         bool exhausted = q >= G.q_end;
-        uint32_t n_rays = exhausted ? 0u : *(volatile const uint32_t*)&queues[q].counters[0];
+        uint32_t front = exhausted ? 0u : *(volatile const uint32_t*)&queues[q].counters[0];
+        uint32_t n_rays = exhausted ? 0u : front + *(volatile const uint32_t*)&queues[q].counters[2];
         bool active = false;
         uint32_t phase = kClear, lq = 0;
         const float4* rec = nullptr;
@@ -277,7 +280,7 @@ __global__ void __launch_bounds__(128, 8) march_batched_kernel(const MarchGroup*
                     if (!active) {
                         uint32_t idx = base + (uint32_t)__popc(need & ((1u << lane) - 1u));
                         if (idx < n_rays) {
-                            rec = reinterpret_cast<const float4*>(Q.rays + idx);
+                            rec = reinterpret_cast<const float4*>(Q.rays + ray_slot(idx, front, Q.cap));
                             float4 a = __ldg(rec), b = __ldg(rec + 1);
                             m.origin = V3{a.x, a.y, a.z};
                             m.dir = V3{b.x, b.y, b.z};
@@ -289,7 +292,10 @@ __global__ void __launch_bounds__(128, 8) march_batched_kernel(const MarchGroup*
                     if (base + cnt >= n_rays) {  // this queue is used up: the next view's
                         q++;
                         if (q >= G.q_end) exhausted = true;
-                        else n_rays = *(volatile const uint32_t*)&queues[q].counters[0];
+                        else {
+                            front = *(volatile const uint32_t*)&queues[q].counters[0];
+                            n_rays = front + *(volatile const uint32_t*)&queues[q].counters[2];
+                        }
                     }
                 }
             }
