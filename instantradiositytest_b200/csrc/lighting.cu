@@ -332,10 +332,11 @@ __global__ void __launch_bounds__(256) shade_kernel(const __grid_constant__ irt_
 // spatial_direct + spatial_indirect, then the resolve passes up to their
 // visibility call: the pixel's contribution value * normalization is stored
 // and, where the reference would march, a ray is appended to the queue
-// (warp-aggregated: one atomic per warp).  Lanes of out-of-image pixels stay
-// in the warp until the append so every ballot sees all 32 lanes.  A warp's
-// light rays are stored first, then its VPL rays, so that neighbouring queue
-// entries take the same phases in the march (a VPL ray has one more
+// (warp-aggregated: one atomic per ray class per warp).  Lanes of
+// out-of-image pixels stay in the warp until the append so every ballot sees
+// all 32 lanes.  VPL rays fill the queue from the front and light rays from
+// the back (ray_slot), so the march takes whole runs of one class and
+// neighbouring queue entries take the same phases (a VPL ray has one more
 // clearance query); each ray's result slot is in its record, so the order
 // changes no result.  The records' fields stay in registers (no indexed
 // local array).
