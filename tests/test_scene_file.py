@@ -253,6 +253,22 @@ def test_missing_fields_types_and_syntax(tmp_path, demo):
     assert error_of(str(tmp_path / "none.json")).startswith("reading ")
 
 
+def test_json_strings_duplicates_and_nesting(tmp_path, demo):
+    # \u escapes (json.dump writes the e-acute as one) decode to the id the
+    # diagnostics print, and an escaped backslash stays one backslash
+    p = mutated(tmp_path, demo, lambda d: d["objects"][0].update(mesh="caf\u00e9\\x"))
+    assert "\\u00e9" in open(p).read()
+    assert "missing mesh caf\u00e9\\x" in error_of(p)
+    # a key given twice and nesting deeper than serde_json's 128 levels are syntax errors
+    txt = open(demo).read()
+    dup = tmp_path / "dup.json"
+    dup.write_text(txt.replace('"version": 1,', '"version": 1, "version": 1,', 1))
+    assert "duplicate field `version`" in error_of(str(dup))
+    deep = tmp_path / "deep.json"
+    deep.write_text(txt.replace('"version": 1,', '"version": 1, "x": ' + "[" * 200 + "]" * 200 + ",", 1))
+    assert "recursion limit" in error_of(str(deep))
+
+
 def test_defaults_and_unknown_fields_are_accepted(tmp_path, demo):
     def edit(d):
         for m in d["materials"]:
