@@ -1,13 +1,15 @@
 """Property tests of the CUDA SVGF and lighting passes, the checks the
 reference runs on its own GPU path (src/gpu_tests.rs:79-181 SVGF noise,
 edges, disocclusion and HDR range; :183-252 history, lights off and debug
-invalidation), on the procedural room instead of the missing exported
-test scene.
+invalidation), on the procedural room and, where IRT_TEST_SCENE names the
+shipped assets/test_scene/scene.json, on the scene those tests load, at
+their 160x100 and settings.json's 100 VPL paths.
 
 As Renderer::test_svgf_signal (src/renderer.rs:557-640) does, a known signal
 replaces the noisy lighting image of a frame before the SVGF passes run.
 """
 import ctypes as C
+import os
 
 import numpy as np
 import pytest
@@ -20,6 +22,19 @@ from instantradiositytest_b200.workload import Workload
 pytestmark = pytest.mark.gpu
 
 W, H = 160, 100
+SHIPPED = os.environ.get("IRT_TEST_SCENE", "")
+SCENES = ["room"] + (["test_scene"] if SHIPPED and os.path.exists(SHIPPED) else [])
+
+
+@pytest.fixture(params=SCENES)
+def scene(request):
+    return request.param
+
+
+def make_workload(scene):
+    if scene == "room":
+        return Workload(0, width=W, height=H)
+    return Workload.load(SHIPPED, width=W, height=H, vpl_count=100)
 
 
 def xorshift_signal(state, n):
@@ -38,8 +53,8 @@ class Rig:
     """One session over the 160x100 room; each frame runs the lighting
     passes, optionally overwrites the noisy image, then the SVGF passes."""
 
-    def __init__(self, moments_format=L.MOMENTS_F32, radiance_format=L.RADIANCE_F32):
-        self.wl = Workload(0, width=W, height=H)
+    def __init__(self, moments_format=L.MOMENTS_F32, radiance_format=L.RADIANCE_F32, scene="room"):
+        self.wl = make_workload(scene)
         self.drv = FrameDriver(self.wl, radiance_format=radiance_format, moments_format=moments_format)
         self.generation = 1
         self.prev_generation = 0
@@ -90,8 +105,8 @@ class Rig:
 
 
 @pytest.mark.parametrize("moments_format", [L.MOMENTS_F32, L.MOMENTS_F16])
-def test_binary_noise_removed_mean_preserved(cuda, moments_format):
-    rig = Rig(moments_format)
+def test_binary_noise_removed_mean_preserved(cuda, moments_format, scene):
+    rig = Rig(moments_format, scene=scene)
     state = 123456789
     for _ in range(12):
         state, sig = xorshift_signal(state, W * H)
@@ -111,8 +126,8 @@ def test_binary_noise_removed_mean_preserved(cuda, moments_format):
     rig.close()
 
 
-def test_material_edge_is_preserved(cuda):
-    rig = Rig()
+def test_material_edge_is_preserved(cuda, scene):
+    rig = Rig(scene=scene)
     for _ in range(3):
         rig.frame()
     # scene.changed(): the signal frame is the first of a new generation, so
@@ -137,8 +152,8 @@ def test_material_edge_is_preserved(cuda):
     rig.close()
 
 
-def test_out_of_bounds_reprojection_restarts_history(cuda):
-    rig = Rig()
+def test_out_of_bounds_reprojection_restarts_history(cuda, scene):
+    rig = Rig(scene=scene)
     for _ in range(4):
         rig.frame()
 
@@ -154,8 +169,8 @@ def test_out_of_bounds_reprojection_restarts_history(cuda):
 
 
 @pytest.mark.parametrize("moments_format", [L.MOMENTS_F32, L.MOMENTS_F16])
-def test_hdr_signal_stays_finite(cuda, moments_format):
-    rig = Rig(moments_format)
+def test_hdr_signal_stays_finite(cuda, moments_format, scene):
+    rig = Rig(moments_format, scene=scene)
     for _ in range(2):
         rig.frame()
     rig.changed()
@@ -173,8 +188,8 @@ def test_hdr_signal_stays_finite(cuda, moments_format):
     rig.close()
 
 
-def test_history_matures_on_static_room(cuda):
-    rig = Rig()
+def test_history_matures_on_static_room(cuda, scene):
+    rig = Rig(scene=scene)
     for _ in range(40):
         rig.frame()
     s = rig.drv.session
@@ -192,8 +207,8 @@ def test_history_matures_on_static_room(cuda):
     rig.close()
 
 
-def test_lights_off_is_black_immediately(cuda):
-    rig = Rig()
+def test_lights_off_is_black_immediately(cuda, scene):
+    rig = Rig(scene=scene)
     for _ in range(6):
         rig.frame()
     assert rig.drv.session.image_host(L.BUF_FILTERED)[..., :3].max() > 0
@@ -209,9 +224,9 @@ def test_lights_off_is_black_immediately(cuda):
     rig.close()
 
 
-def test_history_flag_cleared_restarts_svgf(cuda):
+def test_history_flag_cleared_restarts_svgf(cuda, scene):
     # flags.x = 0 when the debug mode changes (src/renderer.rs:1729)
-    rig = Rig()
+    rig = Rig(scene=scene)
     for _ in range(6):
         rig.frame()
     assert rig.drv.session.moments_host()[..., 2].max() > 1
