@@ -74,6 +74,46 @@ def test_inverse_square_and_spot_cone(cuda):
     ctx.close()
 
 
+def test_inverse_square_and_spot_cone_on_the_cube_fixture(cuda, tmp_path):
+    """src/gpu_tests.rs:281-317 on its own fixture, recreated as a scene file
+    and loaded through Workload.load: the exporter's cube (a 2 m box at the
+    origin, tools/test_export.py), camera at (0, 0, 5) looking down -z, a
+    point light at (0, 0, 3) then (0, 0, 6) — 2 and 5 m from the lit face —
+    then a spot of angle 0.4 aimed down, then up; 64x64, direct light."""
+    from instantradiositytest_b200 import scene_file as sf
+
+    sc = sf.Scene()
+    sc.meshes = [sf.box("Cube", (-1, -1, -1), (1, 1, 1), resolution=16)]
+    sc.materials = [sf.material("Material", (0.8, 0.8, 0.8), 0.5, 0.0)]
+    sc.objects = [sf.obj("Cube", "Cube", "Material")]
+    sc.lights = [sf.point_light("Light", (0, 0, 3), (1, 1, 1), 10.0)]
+    sc.camera = {"position": [0.0, 0.0, 5.0], "rotation": [0.0, 0.0, 0.0, 1.0], "fov_y_radians": 0.6911,
+                 "near": 0.1, "far": 100.0}
+    wl = Workload.load(sf.write_scene(str(tmp_path), sc), width=64, height=64, vpl_count=100)
+    ctx = Context()
+    f, obj, nodes, lights = wl.frame(0)
+    planes = wl.gbuffer_cpu(f, L.GBUFFER_F32)
+    assert planes["depth"][32, 32] < 1.0 and planes["normal"][32, 32][2] > 0.99  # the top face
+
+    def light(z, spot=False, down=True):
+        rec = np.zeros((), L.LIGHT_DTYPE)
+        rec[...] = lights[0]
+        rec["position_strength"] = (0.0, 0.0, z, float(lights[0]["position_strength"][3]))
+        if spot:
+            rec["direction_angle"] = (0.0, 0.0, -1.0 if down else 1.0, 0.4)
+            rec["color_type"][3] = 1.0
+        return rec
+
+    near = centre_radiance(ctx, wl, f, obj, nodes, light(3.0), planes)
+    far = centre_radiance(ctx, wl, f, obj, nodes, light(6.0), planes)
+    print("cube fixture: near", near, "far", far, "ratio", near / far)
+    assert near > 0
+    assert abs(near / far - 6.25) < 0.05, "distance 2 versus 5 must attenuate by 25/4"
+    assert abs(centre_radiance(ctx, wl, f, obj, nodes, light(6.0, spot=True), planes) - far) < 0.002
+    assert centre_radiance(ctx, wl, f, obj, nodes, light(6.0, spot=True, down=False), planes) == 0.0
+    ctx.close()
+
+
 def _world_aabb(model16, lo, hi):
     """World AABB of the SDF-bounds corners under a column-major model (f32,
     the arithmetic of Workload::frame_data / src/renderer.rs:388-400)."""
