@@ -1,5 +1,6 @@
-"""Direct lighting falloff and the spot cone (src/gpu_tests.rs:281-317 on the
-exported analytic cube, here on the procedural room): a point light on the
+"""Direct lighting falloff, the spot cone and a moving occluder
+(src/gpu_tests.rs:281-352) on the reference's exported cube fixture,
+recreated as a scene file, and on the procedural room: a point light on the
 normal of the surface seen at the image centre, at 1 and at 2.5 units (the
 reference's 2 and 5 would leave the room), gives radiance in the ratio 25/4; a spot of half-angle 0.2 rad aimed at the point
 gives the point light's radiance, aimed away gives zero."""
@@ -127,6 +128,61 @@ def _world_aabb(model16, lo, hi):
     return pts.min(0), pts.max(0)
 
 
+def _moved(wl, obj, k, scale, pos):
+    """The objects with object k placed at `pos` with uniform `scale` (no
+    rotation), packed as objects() does, and the rebuilt hierarchy."""
+    mesh, material = int(obj["info"][k, 0]), int(obj["info"][k, 1])
+    lo, hi = wl.meshes[mesh]["lo"][:3].copy(), wl.meshes[mesh]["hi"][:3].copy()
+    model = L.Mat4()
+    vals = [scale, 0, 0, 0, 0, scale, 0, 0, 0, 0, scale, 0, pos[0], pos[1], pos[2], 1.0]
+    for i, x in enumerate(vals):
+        model.m[i] = x
+    moved = obj.copy()
+    rec = np.zeros(1, L.OBJECT_DTYPE)
+    L.lib.irt_pack_object(C.byref(model), C.byref(model), mesh, material, (C.c_float * 3)(*lo), (C.c_float * 3)(*hi),
+                          int(wl.meshes[mesh]["field"][3]), L.ptr(rec))
+    moved[k] = rec[0]
+    los, his = [], []
+    for i in range(len(moved)):
+        mi = int(moved["info"][i, 0])
+        a, b = _world_aabb(moved["model"][i], wl.meshes[mi]["lo"][:3], wl.meshes[mi]["hi"][:3])
+        los.append(a)
+        his.append(b)
+    los = np.ascontiguousarray(np.array(los, np.float32))
+    his = np.ascontiguousarray(np.array(his, np.float32))
+    new_nodes = np.zeros(2 * len(moved) - 1, L.NODE_DTYPE)
+    assert L.lib.irt_build_hierarchy(L.ptr(los), L.ptr(his), len(moved), L.ptr(new_nodes)) == L.IRT_OK
+    return moved, new_nodes
+
+
+def test_moving_occluder_on_the_cube_fixture(cuda, tmp_path):
+    """src/gpu_tests.rs:319-352 on its fixture, recreated as a scene file: a
+    copy of the cube scaled by 0.25 at (20, 0, 2), the point light at
+    (3, 0, 3); moving the copy to (1.5, 0, 2), into the light ray of the
+    centre pixel, makes it dark."""
+    from instantradiositytest_b200 import scene_file as sf
+
+    sc = sf.Scene()
+    sc.meshes = [sf.box("Cube", (-1, -1, -1), (1, 1, 1), resolution=16)]
+    sc.materials = [sf.material("Material", (0.8, 0.8, 0.8), 0.5, 0.0)]
+    sc.objects = [sf.obj("Cube", "Cube", "Material"),
+                  sf.obj("moving_occluder", "Cube", "Material", (20.0, 0.0, 2.0), scale=0.25)]
+    sc.lights = [sf.point_light("Light", (3, 0, 3), (1, 1, 1), 10.0)]
+    sc.camera = {"position": [0.0, 0.0, 5.0], "rotation": [0.0, 0.0, 0.0, 1.0], "fov_y_radians": 0.6911,
+                 "near": 0.1, "far": 100.0}
+    wl = Workload.load(sf.write_scene(str(tmp_path), sc), width=64, height=64, vpl_count=100, vpl_bounces=1)
+    ctx = Context()
+    f, obj, nodes, lights = wl.frame(0)
+    planes = wl.gbuffer_cpu(f, L.GBUFFER_F32)
+    lit = centre_radiance(ctx, wl, f, obj, nodes, lights[0], planes)
+    assert lit > 0.001
+    moved, new_nodes = _moved(wl, obj, 1, 0.25, (1.5, 0.0, 2.0))
+    dark = centre_radiance(ctx, wl, f, moved, new_nodes, lights[0], planes)
+    print("cube fixture: lit", lit, "occluded", dark)
+    assert dark == 0.0, "moving a uniformly scaled occluder into the light ray must update the SDF hierarchy"
+    ctx.close()
+
+
 def test_moving_occluder_updates_the_hierarchy(cuda):
     """src/gpu_tests.rs:319-352: moving a uniformly scaled object into the
     light ray darkens the point — the BVH, the march records and the
@@ -146,29 +202,7 @@ def test_moving_occluder_updates_the_hierarchy(cuda):
     lit = centre_radiance(ctx, wl, f, obj, nodes, light, planes)
     assert lit > 0
     # move the last object (a sphere) to the middle of the ray, scaled by 0.25
-    k = len(obj) - 1
-    mesh, material = int(obj["info"][k, 0]), int(obj["info"][k, 1])
-    lo, hi = wl.meshes[mesh]["lo"][:3].copy(), wl.meshes[mesh]["hi"][:3].copy()
-    mid = p + n * 1.25
-    model = L.Mat4()
-    vals = [0.25, 0, 0, 0, 0, 0.25, 0, 0, 0, 0, 0.25, 0, mid[0], mid[1], mid[2], 1.0]
-    for i, x in enumerate(vals):
-        model.m[i] = x
-    moved = obj.copy()
-    rec = np.zeros(1, L.OBJECT_DTYPE)
-    L.lib.irt_pack_object(C.byref(model), C.byref(model), mesh, material, (C.c_float * 3)(*lo), (C.c_float * 3)(*hi),
-                          int(wl.meshes[mesh]["field"][3]), L.ptr(rec))
-    moved[k] = rec[0]
-    los, his = [], []
-    for i in range(len(moved)):
-        mi = int(moved["info"][i, 0])
-        a, b = _world_aabb(moved["model"][i], wl.meshes[mi]["lo"][:3], wl.meshes[mi]["hi"][:3])
-        los.append(a)
-        his.append(b)
-    los = np.ascontiguousarray(np.array(los, np.float32))
-    his = np.ascontiguousarray(np.array(his, np.float32))
-    new_nodes = np.zeros(2 * len(moved) - 1, L.NODE_DTYPE)
-    assert L.lib.irt_build_hierarchy(L.ptr(los), L.ptr(his), len(moved), L.ptr(new_nodes)) == L.IRT_OK
+    moved, new_nodes = _moved(wl, obj, len(obj) - 1, 0.25, p + n * 1.25)
     dark = centre_radiance(ctx, wl, f, moved, new_nodes, light, planes)
     print("lit", lit, "occluded", dark)
     assert dark == 0.0
