@@ -2,6 +2,7 @@
 generator on the same frames, and the path-budget / source-power invariants
 of src/gpu_tests.rs:354-407 on the device."""
 import ctypes as C
+import os
 
 import numpy as np
 import pytest
@@ -46,8 +47,18 @@ def test_cuda_vpls_match_cpu_generator(cuda, preset, frames):
     ctx.close()
 
 
-def test_cuda_vpl_budget_and_power_normalization(cuda):
-    wl = Workload(0, width=64, height=40)
+SHIPPED = os.environ.get("IRT_TEST_SCENE", "")
+
+
+@pytest.mark.parametrize("scene", ["room"] + (["test_scene"] if SHIPPED and os.path.exists(SHIPPED) else []))
+def test_cuda_vpl_budget_and_power_normalization(cuda, scene):
+    """src/gpu_tests.rs:354-407 — on the procedural room, and on the shipped
+    test scene it was written for (16x16, settings.json's 100 paths) where
+    IRT_TEST_SCENE names it."""
+    if scene == "room":
+        wl = Workload(0, width=64, height=40)
+    else:
+        wl = Workload.load(SHIPPED, width=16, height=16, vpl_count=100)
     ctx = Context()
     scene = Scene(ctx, wl.meshes, wl.atlas, wl.sdf_format)
     f, obj, nodes, lights = wl.frame(0)
