@@ -106,6 +106,13 @@ def test_loaded_scene_mixed_precision_lockstep(cuda, demo):
              radiance_format=L.RADIANCE_F16, moments_format=L.MOMENTS_F16)
 
 
+@pytest.mark.parametrize("schedule", [0, 2])
+def test_loaded_scene_other_schedules_lockstep(cuda, demo, schedule):
+    """The one-kernel-per-entry-point (0) and fused-inline (2) schedules on a
+    loaded scene, with the reference's own Rgba16Float G-buffer targets."""
+    lockstep(demo, 160, 100, 256, 5, gbuffer_format=L.GBUFFER_F16, fused=schedule)
+
+
 def test_batched_views_of_a_loaded_scene_equal_alone(cuda, demo):
     """A batch over a loaded scene and a procedural room (views of uneven
     size, two views of the loaded scene): every view's outputs equal
