@@ -113,6 +113,12 @@ def parse():
     ap.add_argument("--reference-seconds", type=float, default=150.0, help="CPU budget of the reference arm")
     ap.add_argument("--serve-seconds", type=float, default=6.0, help="arrival window of the serving workload")
     ap.add_argument("--serve-streams", type=int, default=2)
+    ap.add_argument("--field-filter", type=int, default=0, choices=[0, 1],
+                    help="SDF sampler: 0 point-sampled trilinear (default), 1 the reference's hardware-filtered one")
+    ap.add_argument("--no-headline", action="store_true",
+                    help="skip the mixed-precision and served-vs-plain runs the default line carries")
+    ap.add_argument("--headline-serve-seconds", type=float, default=3.0,
+                    help="arrival window of the served-vs-plain run in the default line")
     return ap.parse_args()
 
 
@@ -394,6 +400,86 @@ def reference_arm(args):
 
 
 # ------------------------------------------------------------------ our arm
+class DeviceRun:
+    """One session over a workload with every frame's inputs resident in HBM
+    before timing: a distinct G-buffer per frame from the CUDA producer and
+    the VPL pool of each frame.  timed() renders `warmup` frames, then times
+    `steps` frames with CUDA events on the stream (with per-stage events in
+    the session), sampling SM clocks meanwhile."""
+
+    def __init__(self, ctx, wl, gfmt, rfmt, mfmt, schedule, n_frames, field_filter=0):
+        import ctypes as C
+
+        import torch
+
+        from instantradiositytest_b200 import _lib as L
+        from instantradiositytest_b200.runtime import Scene, Session, gbuffer_device_alloc, session_desc, stream_handle
+
+        self.C, self.torch, self.L = C, torch, L
+        self.ctx, self.wl = ctx, wl
+        self.scene = Scene(ctx, wl.meshes, wl.atlas, wl.sdf_format)
+        self.scene.set_field_filter(field_filter)
+        self.sess = Session(ctx, session_desc(wl.settings, gfmt, rfmt, schedule, False, moments_format=mfmt))
+        self.sh = stream_handle()
+        self.frames, self.gbufs, self.vpls = [], [], []
+        for i in range(n_frames):
+            f, obj, nodes, lights = wl.frame(i)
+            t, gs = gbuffer_device_alloc(wl.height, wl.width, gfmt)
+            L.check(L.lib.irt_gbuffer_render(ctx.handle, wl.handle, C.byref(f), None, gfmt, gs.depth,
+                                             gs.normal, gs.color, gs.params, gs.motion, self.sh), ctx.handle, "gbuffer")
+            v = wl.vpls_cpu(f, obj, lights)
+            self.frames.append((f, obj, nodes, lights))
+            self.gbufs.append((t, gs))
+            self.vpls.append(torch.from_numpy(v.view(np.uint8)).cuda())
+        torch.cuda.synchronize()
+        self.zero_vpls = torch.zeros_like(self.vpls[0])
+
+    def render(self, i):
+        C = self.C
+        f, obj, nodes, lights = self.frames[i]
+        self.scene.update(obj, nodes, lights, self.sh)
+        prev = self.vpls[i - 1] if i > 0 else self.zero_vpls
+        self.sess.render(self.scene, f, self.gbufs[i][1], C.c_void_p(self.vpls[i].data_ptr()),
+                         C.c_void_p(prev.data_ptr()), self.sh)
+
+    def timed(self, warmup, steps, dist=None, device=0):
+        torch = self.torch
+        stream = torch.cuda.current_stream()
+        clocks = Clocks(device)
+        clocks.start()  # sampling runs from the warm-up on; samples are kept for the timed span
+        for i in range(warmup):
+            self.render(i)
+        torch.cuda.synchronize()
+        if dist:
+            dist.barrier()
+        self.sess.set_profiling(True)
+        torch.cuda.synchronize()
+        if dist:
+            dist.barrier()
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        t_start = time.time()
+        e0.record(stream)
+        for i in range(warmup, warmup + steps):
+            self.render(i)
+        e1.record(stream)
+        torch.cuda.synchronize()
+        t_end = time.time()
+        if dist:
+            dist.barrier()
+        clk = clocks.stop(t_start, t_end)
+        ring0 = max(warmup, warmup + steps - 128)  # the session keeps events of the last 128 frames
+        stage = np.array([self.sess.pass_ms(i) for i in range(ring0, warmup + steps)])  # [frames, 10]
+        self.sess.set_profiling(False)
+        assert self.sess.check() == self.L.IRT_OK, self.ctx.error()
+        return {"ms": e0.elapsed_time(e1), "stage": stage, "clocks": clk}
+
+    def close(self):
+        self.sess.close()
+        self.scene.close()
+        self.gbufs.clear()
+        self.vpls.clear()
+
+
 def ours(args):
     import ctypes as C
 
@@ -420,61 +506,15 @@ def ours(args):
     K, Wm = args.steps, args.warmup
     n_frames = K + Wm
     ctx = Context(dev)
-    scene = Scene(ctx, wl.meshes, wl.atlas, wl.sdf_format)
     schedule = args.schedule
     gfmt, rfmt, mfmt, storage = storage_of(args.config)
     alg = alg_bytes(gfmt, rfmt, mfmt)
-    sess = Session(ctx, session_desc(wl.settings, gfmt, rfmt, schedule, False, moments_format=mfmt))
+    run = DeviceRun(ctx, wl, gfmt, rfmt, mfmt, schedule, n_frames, args.field_filter)
+    scene, sess, frames = run.scene, run.sess, run.frames
     stream = torch.cuda.current_stream()
     sh = stream_handle()
-
-    # ---- inputs resident in HBM: per-frame G-buffers (CUDA producer) and VPLs
-    frames, gbufs, vpls = [], [], []
-    for i in range(n_frames):
-        f, obj, nodes, lights = wl.frame(i)
-        t, gs = gbuffer_device_alloc(H, W, gfmt)
-        L.check(L.lib.irt_gbuffer_render(ctx.handle, wl.handle, C.byref(f), None, gfmt, gs.depth,
-                                         gs.normal, gs.color, gs.params, gs.motion, sh), ctx.handle, "gbuffer")
-        v = wl.vpls_cpu(f, obj, lights)
-        frames.append((f, obj, nodes, lights))
-        gbufs.append((t, gs))
-        vpls.append(torch.from_numpy(v.view(np.uint8)).cuda())
-    torch.cuda.synchronize()
-    zero_vpls = torch.zeros_like(vpls[0])
-
-    def render(i):
-        f, obj, nodes, lights = frames[i]
-        scene.update(obj, nodes, lights, sh)
-        prev = vpls[i - 1] if i > 0 else zero_vpls
-        sess.render(scene, f, gbufs[i][1], C.c_void_p(vpls[i].data_ptr()), C.c_void_p(prev.data_ptr()), sh)
-
-    clocks = Clocks(dev)
-    clocks.start()  # sampling runs from the warm-up on; samples are kept for the timed span
-    for i in range(Wm):
-        render(i)
-    torch.cuda.synchronize()
-    if dist:
-        dist.barrier()
-    sess.set_profiling(True)
-    torch.cuda.synchronize()
-    if dist:
-        dist.barrier()
-    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
-    t_start = time.time()
-    e0.record(stream)
-    for i in range(Wm, Wm + K):
-        render(i)
-    e1.record(stream)
-    torch.cuda.synchronize()
-    t_end = time.time()
-    if dist:
-        dist.barrier()
-    clk = clocks.stop(t_start, t_end)
-    ms = e0.elapsed_time(e1)
-    ring0 = max(Wm, Wm + K - 128)  # the session keeps events of the last 128 frames
-    stage = np.array([sess.pass_ms(i) for i in range(ring0, Wm + K)])  # [K, 10]
-    sess.set_profiling(False)
-    assert sess.check() == L.IRT_OK, ctx.error()
+    timed = run.timed(Wm, K, dist, dev)
+    ms, stage, clk = timed["ms"], timed["stage"], timed["clocks"]
     value, ms_max = replica_value(P, K, ms, world, dist)
     frame_ms = stage[:, 9]
     names = STAGES
@@ -549,20 +589,31 @@ def ours(args):
     march_flops = None
     if counters:
         march_flops = sum(FLOPS_PER[k] * counters.get(k, 0.0) for k in FLOPS_PER)
-    roofline = {"bound": "hbm", "kernel": dominant, "achieved": ach(dominant), "peak": peak, "unit": "GB/s",
-                "frac": ach(dominant) / peak, "traffic": ncu_traffic(dominant, f"{W}x{H}" + ("_mixed" if args.config == 2 else "")), "peak_source": peak_kind,
-                "alg_bytes_per_pixel": alg[dominant],
-                "kernels": {n: {"ms": float(mean_ms[kernel_idx[n]]), "alg_GBps": ach(n), "frac": ach(n) / peak}
-                            for n in KERNELS}}
-    if march_flops is not None:
+    traffic = ncu_traffic(dominant, f"{W}x{H}" + ("_mixed" if args.config == 2 else ""))
+    kernels = {n: {"ms": float(mean_ms[kernel_idx[n]]), "alg_GBps": ach(n), "frac": ach(n) / peak} for n in KERNELS}
+    hbm = {"achieved": ach(dominant), "peak": peak, "unit": "GB/s", "frac": ach(dominant) / peak,
+           "peak_source": peak_kind, "alg_bytes_per_pixel": alg[dominant]}
+    if dominant == "march" and march_flops is not None:
+        # The march is bound by FP32 issue under divergence, not by memory:
+        # its roofline is the counted FP32 work against the FP32 SIMT peak.
         t = mean_ms[kernel_idx["march"]] / 1000.0
-        roofline["march_fp32"] = {
-            "flops_per_pixel": march_flops, "achieved_tflops": march_flops * P / t / 1e12,
-            "peak_tflops": FP32_PEAK_TFLOPS, "peak_source": "nominal (148 SMs x 128 FP32 lanes x 2 x 1.965 GHz)",
-            "frac": march_flops * P / t / 1e12 / FP32_PEAK_TFLOPS,
-            "counters_per_pixel": counters,
-            "note": "the march is FP32/latency bound; flops counted by the oracle on a band of the same frame"}
+        tflops = march_flops * P / t / 1e12
+        roofline = {"bound": "fp32", "kernel": "march", "achieved": tflops, "peak": FP32_PEAK_TFLOPS,
+                    "unit": "TFLOP/s", "frac": tflops / FP32_PEAK_TFLOPS, "traffic": traffic,
+                    "peak_source": "nominal FP32 SIMT peak (148 SMs x 128 lanes x 2 flops x 1.965 GHz); "
+                                   "MEASURED_PEAKS.json holds no FP32 figure",
+                    "flops_per_pixel": march_flops, "flops_model": FLOPS_PER, "counters_per_pixel": counters,
+                    "flops_note": "oracle work counters of a band of the same frame weighted by FLOPS_PER",
+                    "hbm": hbm, "kernels": kernels}
+    else:
+        roofline = dict(bound="hbm", kernel=dominant, traffic=traffic, kernels=kernels, **hbm)
 
+    # ---- the headline comparison: mixed-precision storage, the reference's
+    # filtered field sampler, and the served form against the plain one
+    headline = None
+    if rank == 0 and world == 1 and args.config == 1 and not args.scene and not args.no_headline:
+        run.close()  # frees this run's per-frame inputs first
+        headline = headline_runs(ctx, dev, schedule, value, frame_ms, args)
     if rank == 0:
         line = {
             "metric": "Mpix-frames/s", "value": value, "unit": "Mpix-frames/s", "n_gpus": world, "steps": K,
@@ -576,13 +627,64 @@ def ours(args):
             "gpu_launches": K * KERNELS_PER_FRAME[schedule],
             "clocks": clk,
         }
+        if args.field_filter:
+            line["config"]["field_filter"] = "hardware linear (the reference's filtered sample_field)"
+        if headline is not None:
+            line["headline"] = headline
         print(json.dumps(line), flush=True)
-    sess.close()
-    scene.close()
+    run.close()
     ctx.close()
     if dist:
         dist.barrier()
         dist.destroy_process_group()
+
+
+def headline_runs(ctx, dev, schedule, plain_value, plain_frame_ms, args):
+    """The comparison the headline metric names, on one GPU: the plain
+    single-view path (this line's value: 1920x1200, f32 storage) beside
+    (1) the same room with mixed-precision storage, (2) the same room with
+    the reference's hardware-filtered SDF sampler, each device-timed over
+    60 frames after 8 warm-up frames, and (3) the serving workload's
+    served form against the same requests run session by session, over a
+    short arrival window (the configured workload is 4/s over 120 s)."""
+    from instantradiositytest_b200.workload import Workload
+
+    K, Wm = 60, 8
+    out = {"plain": {"value": plain_value, "p50_frame_ms": float(np.percentile(plain_frame_ms, 50)),
+                     "p99_frame_ms": float(np.percentile(plain_frame_ms, 99)),
+                     "workload": "1920x1200 room of 24 meshes, f32 storage (this line's value)"}}
+    for key, preset, field_filter, what in (
+            ("mixed", 2, 0, "same room and frames, packed G-buffer, f16 SDF / radiance / moments"),
+            ("field_linear", 1, 1, "same room, f32 storage, the reference's hardware-filtered sample_field")):
+        wl = Workload(preset)
+        gfmt, rfmt, mfmt, _ = storage_of(preset)
+        run = DeviceRun(ctx, wl, gfmt, rfmt, mfmt, schedule, K + Wm, field_filter)
+        t = run.timed(Wm, K, None, dev)
+        run.close()
+        P = wl.width * wl.height
+        wl.close()
+        fm = t["stage"][:, 9]
+        out[key] = {"value": P * K / (t["ms"] / 1000.0) / 1e6, "ms_per_step": t["ms"] / K,
+                    "p50_frame_ms": float(np.percentile(fm, 50)), "p99_frame_ms": float(np.percentile(fm, 99)),
+                    "march_ms": float(t["stage"][:, 3].mean()), "steps": K, "warmup": Wm, "clocks": t["clocks"],
+                    "workload": what}
+        out[key]["over_plain"] = out[key]["value"] / plain_value
+    reqs, served, plain, t_build, _ = serve_measure(args.headline_serve_seconds, args.serve_streams)
+    keep = ("mpix_frames_per_s", "frames", "sessions", "seconds", "p50_latency_ms", "p99_latency_ms",
+            "p50_frame_ms", "p99_frame_ms", "p50_wait_ms", "p99_wait_ms", "mean_active", "peak_active")
+    out["served"] = {k: served[k] for k in keep}
+    out["served"]["clocks"] = served["clocks"]
+    out["served_plain_arm"] = {k: plain[k] for k in keep}
+    out["served"]["over_plain_arm"] = served["mpix_frames_per_s"] / max(plain["mpix_frames_per_s"], 1e-9)
+    out["served"]["over_plain_1920x1200"] = served["mpix_frames_per_s"] / plain_value
+    out["served"]["workload"] = (f"serving workload: Poisson arrivals 4/s over {args.headline_serve_seconds} s "
+                                 f"({len(reqs)} sessions; configured 120 s), scenes of 8-64 meshes, resolutions "
+                                 f"{SERVE_RESOLUTIONS}, U(30,300) frames paced at 60 fps, mixed-precision storage, "
+                                 f"160 GB admission budget, {args.serve_streams} streams; plain arm: the same "
+                                 f"requests one at a time, unpaced")
+    out["target"] = ("north star: the served/batched FP16-storage form at >= 3x the plain single-view path's "
+                     "Mpix-frames/s; compare served.over_plain_arm and mixed.over_plain")
+    return out
 
 
 # ------------------------------------------------------------------ serving
@@ -606,25 +708,22 @@ def serving_requests(window_s, rate, seed=7):
         i += 1
 
 
-def serve(args):
-    """Serving workload: sessions arriving at 4/s, admitted against a 160 GB
-    budget, frames paced at 60 fps, mixed-precision storage; the same
-    requests then run session by session (one at a time, unpaced) as the
-    plain arm."""
+def serve_measure(window_s, streams, rate=4.0):
+    """The serving workload: Poisson arrivals at `rate`/s over `window_s`
+    seconds (serving_requests), mixed-precision storage, 160 GB admission
+    budget, frames paced at 60 fps, sessions spread over `streams` CUDA
+    streams; then the same requests session by session (one at a time,
+    unpaced) as the plain arm.  Returns (requests, served stats, plain
+    stats, scene build seconds)."""
     from concurrent.futures import ThreadPoolExecutor
 
     import torch
 
-    from instantradiositytest_b200 import _lib as L
     from instantradiositytest_b200.runtime import Context
     from instantradiositytest_b200.serving import Server
     from instantradiositytest_b200.workload import Workload, preset_spec
 
-    rank, world, local = rank_info()
-    torch.cuda.set_device(local if world > 1 else 0)
-    if rank != 0 and world > 1:
-        return
-    reqs = serving_requests(args.serve_seconds, 4.0)
+    reqs = serving_requests(window_s, rate)
 
     def build(r):
         m = r["meshes"]
@@ -642,7 +741,7 @@ def serve(args):
     results = {}
     for arm in ("served", "plain"):
         if arm == "served":
-            srv = Server(ctx, budget, streams=args.serve_streams, frame_rate=60.0, gbuffer_format=gfmt,
+            srv = Server(ctx, budget, streams=streams, frame_rate=60.0, gbuffer_format=gfmt,
                          radiance_format=rfmt, moments_format=mfmt)
             for r, wl in zip(reqs, wls):
                 srv.submit(r["id"], r["arrival_s"], r["frames"], wl)
@@ -660,9 +759,27 @@ def serve(args):
         st["wall_s"] = t1 - t0
         srv.close()
         results[arm] = st
-    served, plain = results["served"], results["plain"]
-    frames = int(served["frames"])
+    ctx.close()
     scene_bytes = float(np.mean([wl.object_count * (208 + 96) + wl.light_count * 48 + 384 for wl in wls]))
+    for wl in wls:
+        wl.close()
+    return reqs, results["served"], results["plain"], t_build, scene_bytes
+
+
+def serve(args):
+    """Serving workload as its own JSON line: sessions
+    arriving at 4/s, admitted against a 160 GB budget, frames paced at
+    60 fps, mixed-precision storage, against the same requests run session
+    by session."""
+    import torch
+
+    rank, world, local = rank_info()
+    torch.cuda.set_device(local if world > 1 else 0)
+    if rank != 0 and world > 1:
+        return
+    reqs, served, plain, t_build, scene_bytes = serve_measure(args.serve_seconds, args.serve_streams)
+    gfmt, rfmt, mfmt, storage = storage_of(2)
+    frames = int(served["frames"])
     line = {
         "metric": "Mpix-frames/s", "value": served["mpix_frames_per_s"], "unit": "Mpix-frames/s", "n_gpus": 1,
         "steps": frames, "warmup": 0, "ms_per_step": 1000.0 * served["seconds"] / max(frames, 1),
@@ -689,7 +806,6 @@ def serve(args):
         "roofline": None, "cpu_baseline": None,
     }
     print(json.dumps(line), flush=True)
-    ctx.close()
 
 
 # ------------------------------------------------------------------ batched views

@@ -201,6 +201,31 @@ irt_status irt_scene_update(irt_scene* scene, const irt_object* objects, uint32_
                             uint32_t light_count, void* stream);
 void irt_scene_destroy(irt_scene* scene);
 
+/* Field sampler of a scene's SDF meshes.
+ *   POINT:  sample_field of common.wgsl:31-38 — the cell's 8 texels loaded
+ *           and weighted in f32 (the default; the reference's path when the
+ *           adapter cannot filter R32Float).
+ *   LINEAR: the reference's filtered variant, src/renderer.rs:277-286 (used
+ *           there whenever FLOAT32_FILTERABLE is present,
+ *           src/renderer.rs:736-739, :914-921, :1470-1471): one hardware
+ *           linear fetch at (origin + q + .5) / atlas_dims through a
+ *           clamp-to-edge linear sampler.  The filter weights are the
+ *           hardware's fixed-point ones (8 fractional bits), which the mesh
+ *           bound's voxel/128 allowance covers (sdf.wgsl:16-17).
+ * irt_scene_set_field_filter takes effect at the scene's next
+ * irt_scene_update (which rebuilds the march's leaf-order cache under the
+ * new sampler). */
+#define IRT_FIELD_POINT 0
+#define IRT_FIELD_LINEAR 1
+irt_status irt_scene_set_field_filter(irt_scene* scene, int32_t filter);
+/* sample_field with `filter` of field mesh `mesh` at n grid-space points
+ * q (device array of 3*n floats, q in [0, res-1]^3 as mesh_distance forms
+ * it, sdf.wgsl:12); out: n floats on the device, dequantised (F16 atlases
+ * times the mesh's scale).  The kernels' own sampler, exposed for parity
+ * tests of the sampler alone; no counterpart in the reference. */
+irt_status irt_scene_sample_field(const irt_scene* scene, int32_t filter, uint32_t mesh, const float* q,
+                                  uint32_t n, float* out, void* stream);
+
 typedef struct irt_session_desc {
     irt_settings settings;
     int32_t gbuffer_format;
@@ -307,19 +332,24 @@ irt_status irt_session_pass_ms_at(irt_session* s, uint32_t frame_index, float ou
  * thread that must not stall on an allocation, or a host that reserves all
  * device memory under its own allocator.  No counterpart in the reference
  * (there the filter's images are Svgf-owned textures).  The caller passes all
- * inputs (the svgf_temporal radiance and moments a session exposes as
- * IRT_BUF_TEMPORAL / IRT_BUF_MOMENTS, or its own) and outputs (filtered
- * image; feedback image of the first pass, may be NULL), in the radiance
- * format given.  The two ping-pong images between passes live in a fixed
- * 8 MiB array of this library's device memory that every GPU loading the
- * library holds until exit; frames above 262144 pixels (512x512) are
- * rejected.  The first call on each device looks up that array's address,
- * so it should come before any stream capture.  All calls share the array:
- * calls that overlap on the GPU race.  No cudaMalloc/cudaFree is called.
- * `err` (may be NULL) receives a message on failure. */
+ * inputs — the svgf_temporal radiance (radiance_format) and moments
+ * (moments_format: IRT_MOMENTS_F32 16-byte or IRT_MOMENTS_F16 8-byte texels),
+ * e.g. a session's IRT_BUF_TEMPORAL and IRT_BUF_MOMENTS with that session's
+ * formats — and outputs (filtered image; feedback image of the first pass,
+ * may be NULL), in the radiance format given.  The frame's positions and
+ * edge-stopping features and the two ping-pong images between passes live in
+ * a fixed 20 MiB array of this library's device memory that every GPU loading
+ * the library holds until exit; frames above 262144 pixels (512x512) are
+ * rejected.  The first call on each device looks up that array's address
+ * (with the device current), so it should come before any stream capture,
+ * and the device must not be reset afterwards while the library is loaded.
+ * All calls share the array: calls that overlap on the GPU race.  No
+ * cudaMalloc/cudaFree is called.  With a session's inputs the outputs equal
+ * the session's own filtered and feedback images bit for bit.  `err` (may be
+ * NULL) receives a message on failure. */
 irt_status irt_svgf_spatial_noalloc(const irt_frame* frame, const irt_gbuffer* gbuffer,
-                                    int32_t radiance_format, uint32_t iterations,
-                                    const void* temporal_radiance, const float* moments,
+                                    int32_t radiance_format, int32_t moments_format, uint32_t iterations,
+                                    const void* temporal_radiance, const void* moments,
                                     void* filtered_out, void* feedback_out, void* stream,
                                     char* err, size_t err_len);
 
@@ -529,6 +559,9 @@ typedef struct irt_request {
     irt_workload* workload;     /* scene + camera path; caller-owned, outlives the run */
     uint32_t capture_frame;     /* frame whose filtered image is copied ...     */
     void* capture;              /* ... to this host buffer (NULL = none)        */
+    double* times;              /* NULL, or 3 doubles written by irt_server_run:
+                                   admitted, last frame done, retired (seconds
+                                   after the run starts; -1 if never admitted) */
 } irt_request;
 
 typedef struct irt_server_stats {

@@ -27,6 +27,7 @@ GBUFFER_F32, GBUFFER_F16, GBUFFER_PACKED = 0, 1, 2
 RADIANCE_F32, RADIANCE_F16 = 0, 1
 MOMENTS_F32, MOMENTS_F16 = 0, 1
 SDF_F32, SDF_F16 = 0, 1
+FIELD_POINT, FIELD_LINEAR = 0, 1
 
 BUF_DIRECT, BUF_NOISY, BUF_FILTERED, BUF_MOMENTS = 0, 1, 2, 3
 BUF_RES_DIRECT, BUF_RES_INDIRECT, BUF_VPL_ARCHIVE = 4, 5, 6
@@ -114,7 +115,7 @@ class ServerDesc(C.Structure):
 class Request(C.Structure):
     _fields_ = [
         ("id", C.c_uint64), ("arrival_s", C.c_double), ("frames", C.c_uint32), ("workload", C.c_void_p),
-        ("capture_frame", C.c_uint32), ("capture", C.c_void_p),
+        ("capture_frame", C.c_uint32), ("capture", C.c_void_p), ("times", C.POINTER(C.c_double)),
     ]
 
 
@@ -180,8 +181,10 @@ _PROTOS = {
     "irt_session_set_profiling": (I32, [P, I32]),
     "irt_session_pass_ms": (I32, [P, C.POINTER(C.c_float)]),
     "irt_session_pass_ms_at": (I32, [P, U32, C.POINTER(C.c_float)]),
-    "irt_svgf_spatial_noalloc": (I32, [C.POINTER(Frame), C.POINTER(GBuffer), I32, U32, P, P, P, P, P, C.c_char_p,
-                                       C.c_size_t]),
+    "irt_scene_set_field_filter": (I32, [P, I32]),
+    "irt_scene_sample_field": (I32, [P, I32, U32, P, U32, P, P]),
+    "irt_svgf_spatial_noalloc": (I32, [C.POINTER(Frame), C.POINTER(GBuffer), I32, I32, U32, P, P, P, P, P,
+                                       C.c_char_p, C.c_size_t]),
     "irt_is_box_geometry": (I32, [P, U32, P, U32, C.POINTER(C.c_float), C.POINTER(C.c_float)]),
     "irt_field_lipschitz_bound": (C.c_float, [P, U32, C.POINTER(C.c_float)]),
     "irt_mesh_metadata": (I32, [P, U32, P, U32, P, U32, C.POINTER(C.c_float), C.POINTER(C.c_float),

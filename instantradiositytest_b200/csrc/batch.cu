@@ -147,6 +147,7 @@ LightingLaunch lighting_launch(irt_session* s, const irt_scene* sc, const irt_fr
     L.atlas = sc->atlas;
     L.sdf_f16 = sc->sdf_f16;
     L.sdf_cells = sc->sdf_cells;
+    L.field_filter = scene_field_filter(sc);
     L.error = s->error;
     L.cur_vpls = cur;
     L.prev_vpls = prev;
@@ -298,6 +299,7 @@ irt_status build_tables(irt_batch* b, int p, irt_scene* const* scenes, const irt
             G.atlas = sc->atlas;
             G.sdf_f16 = sc->sdf_f16;
             G.sdf_cells = sc->sdf_cells;
+            G.field_filter = scene_field_filter(sc);
             G.march_scene = sc->march_scene;
             const uint32_t bytes = irt_march_scene_bytes(sc->object_count);
             G.scene_vec4 = bytes / 16;

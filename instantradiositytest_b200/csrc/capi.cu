@@ -113,6 +113,12 @@ irt_status irt_scene_create(irt_context* ctx, const irt_mesh* meshes, uint32_t m
     td.normalizedCoords = 0;
     e = cudaCreateTextureObject(&sc->atlas, &rd, &td, nullptr);
     if (e != cudaSuccess) return fail(cuda_fail(ctx, e, "texture object"));
+    // The reference's field_sampler (src/renderer.rs:914-921): linear
+    // min/mag filter, clamp-to-edge, sampled at normalised coordinates.
+    td.filterMode = cudaFilterModeLinear;
+    td.normalizedCoords = 1;
+    e = cudaCreateTextureObject(&sc->atlas_linear, &rd, &td, nullptr);
+    if (e != cudaSuccess) return fail(cuda_fail(ctx, e, "linear texture object"));
     // Corner cells of the field meshes (DevScene::sdf_cells); a mesh's first
     // record index goes into hi[3] of its rows, which nothing else reads.
     {
@@ -282,6 +288,13 @@ irt_status irt_scene_update(irt_scene* sc, const irt_object* objects, uint32_t o
     CK(cudaMemcpyAsync(sc->march_scene, stage_march, mbytes, cudaMemcpyHostToDevice, st), "march scene");
     CK(cudaEventRecord(sc->pinned_free[slot], st), "staging");
     sc->updates++;
+    // A new field sampler changes every object distance the leaf-order cache
+    // bounds, so it takes effect here, with the cache rebuilt.
+    if (sc->field_linear != sc->field_linear_requested) {
+        sc->field_linear = sc->field_linear_requested;
+        sc->cached_nodes.clear();
+        sc->cached_objects.clear();
+    }
     // Leaf-order cache, rebuilt on the device when the BVH or an object
     // changes (static scenes build it once).
     if (sc->cached_nodes.size() != node_count || sc->cached_objects.size() != object_count ||
@@ -313,6 +326,7 @@ irt_status irt_scene_update(irt_scene* sc, const irt_object* objects, uint32_t o
         LC.atlas = sc->atlas;
         LC.sdf_f16 = sc->sdf_f16;
         LC.sdf_cells = sc->sdf_cells;
+        LC.field_filter = scene_field_filter(sc);
         for (int a = 0; a < 3; a++) {
             // The grid covers the root box grown by 0.1 % and 1 mm.
             double ext = (double)nodes[0].hi[a] - (double)nodes[0].lo[a];
@@ -355,10 +369,45 @@ irt_status irt_vpl_generate(irt_scene* sc, const irt_workload* wl, const irt_fra
     return IRT_OK;
 }
 
+irt_status irt_scene_set_field_filter(irt_scene* sc, int32_t filter) {
+    if (!sc) return IRT_E_INVALID;
+    if (filter != IRT_FIELD_POINT && filter != IRT_FIELD_LINEAR) {
+        sc->ctx->set_error("unknown field filter");
+        return IRT_E_INVALID;
+    }
+    sc->field_linear_requested = filter == IRT_FIELD_LINEAR;
+    return IRT_OK;
+}
+
+irt_status irt_scene_sample_field(const irt_scene* sc, int32_t filter, uint32_t mesh, const float* q, uint32_t n,
+                                  float* out, void* stream) {
+    if (!sc) return IRT_E_INVALID;
+    irt_context* ctx = sc->ctx;
+    if ((filter != IRT_FIELD_POINT && filter != IRT_FIELD_LINEAR) || mesh >= sc->mesh_count || !q || !out || !n) {
+        ctx->set_error("sample_field: bad filter, mesh index, points or output");
+        return IRT_E_INVALID;
+    }
+    const irt_mesh& row = sc->host_meshes[mesh];
+    if (row.geometry_lo[3] > .5f) {
+        ctx->set_error("sample_field: the mesh is a certified box and has no field");
+        return IRT_E_INVALID;
+    }
+    DeviceGuard dg(ctx->device);
+    irtd::DevScene d{};
+    d.atlas = sc->atlas;
+    d.sdf_f16 = sc->sdf_f16;
+    d.sdf_cells = sc->sdf_cells;
+    d.filter = scene_field_filter(sc);
+    d.filter.linear = filter == IRT_FIELD_LINEAR ? sc->atlas_linear : 0;
+    CK(irt_launch_sample_field(d, row, q, n, out, static_cast<cudaStream_t>(stream)), "sample_field kernel");
+    return IRT_OK;
+}
+
 void irt_scene_destroy(irt_scene* sc) {
     if (!sc) return;
     DeviceGuard g(sc->ctx->device);
     if (sc->atlas) cudaDestroyTextureObject(sc->atlas);
+    if (sc->atlas_linear) cudaDestroyTextureObject(sc->atlas_linear);
     if (sc->atlas_array) cudaFreeArray(sc->atlas_array);
     if (sc->sdf_cells) cudaFree(sc->sdf_cells);
     if (sc->meshes) cudaFree(sc->meshes);
@@ -597,6 +646,7 @@ irt_status irt_frame_lighting(irt_session* s, const irt_scene* sc, const irt_fra
     L.atlas = sc->atlas;
     L.sdf_f16 = sc->sdf_f16;
     L.sdf_cells = sc->sdf_cells;
+    L.field_filter = scene_field_filter(sc);
     L.error = s->error;
     L.cur_vpls = cur;
     L.prev_vpls = prev;
@@ -634,6 +684,7 @@ irt_status irt_frame_lighting(irt_session* s, const irt_scene* sc, const irt_fra
         M.atlas = sc->atlas;
         M.sdf_f16 = sc->sdf_f16;
         M.sdf_cells = sc->sdf_cells;
+        M.field_filter = scene_field_filter(sc);
         M.error = s->error;
         M.march_scene = sc->march_scene;
         M.cells = sc->cells;

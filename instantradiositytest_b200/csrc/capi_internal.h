@@ -32,6 +32,11 @@ struct irt_scene {
     irt_mesh* meshes = nullptr;
     cudaArray_t atlas_array = nullptr;
     cudaTextureObject_t atlas = 0;
+    // The same atlas through a linear sampler at normalised coordinates, for
+    // the reference's filtered sample_field (IRT_FIELD_LINEAR).
+    cudaTextureObject_t atlas_linear = 0;
+    int field_linear = 0;            // in use since the last irt_scene_update
+    int field_linear_requested = 0;  // irt_scene_set_field_filter, applied by the next update
     int sdf_f16 = 0;
     uint32_t atlas_dims[3] = {0, 0, 0};
     // Corner cells: per field mesh, the 8 corner texels of each of its
@@ -64,6 +69,15 @@ struct irt_scene {
     uint32_t object_count = 0, light_count = 0;
     uint64_t bytes = 0;
 };
+
+// The field sampler the kernels use for a scene (point-sampled trilinear or
+// the hardware-linear fetch).
+inline irtd::FieldFilter scene_field_filter(const irt_scene* sc) {
+    irtd::FieldFilter f{};
+    f.linear = sc->field_linear ? sc->atlas_linear : 0;
+    for (int a = 0; a < 3; a++) f.dims[a] = (float)sc->atlas_dims[a];
+    return f;
+}
 
 struct irt_session {
     irt_context* ctx = nullptr;

@@ -4,6 +4,7 @@
 // and the Quilez soft-shadow march.
 #pragma once
 #include "dev_common.cuh"
+#include "kernels.h"
 
 namespace irtd {
 
@@ -21,6 +22,7 @@ struct DevScene {
     // holding the 8 texels t[k] at (cx + (k&1), cy + (k>>1 & 1), cz + (k>>2))
     // of its atlas tile — two float4 (f32) or eight halves in one uint4 (f16).
     const void* sdf_cells;
+    FieldFilter filter;
 };
 
 // Read-only-path loads of the scene records as 16-byte vectors.
@@ -73,6 +75,15 @@ __device__ __forceinline__ float signed_box_distance(V3 p, V3 lo, V3 hi) {
 // common.wgsl:31-38 — the 8 texels of the cell (clamped to res-2), weights in
 // z, y, x order as the WGSL loop accumulates them.
 __device__ __forceinline__ float sample_field(const DevScene& sc, const DMesh& m, V3 q) {
+    if (sc.filter.linear) {
+        // textureSampleLevel(fields, field_sampler, (vec3<f32>(origin)+q+.5)/vec3<f32>(dims), 0.)
+        // with IEEE rounding in every build, so the coordinate is the reference's.
+        const float u = __fdiv_rn(__fadd_rn(__fadd_rn((float)m.field.x, q.x), .5f), sc.filter.dims[0]);
+        const float v = __fdiv_rn(__fadd_rn(__fadd_rn((float)m.field.y, q.y), .5f), sc.filter.dims[1]);
+        const float w = __fdiv_rn(__fadd_rn(__fadd_rn((float)m.field.z, q.z), .5f), sc.filter.dims[2]);
+        const float value = tex3D<float>(sc.filter.linear, u, v, w);
+        return sc.sdf_f16 ? value * m.lo.w : value;
+    }
     uint32_t res = m.field.w;
     uint32_t cx = min(to_u32(floorf(q.x)), res - 2u);
     uint32_t cy = min(to_u32(floorf(q.y)), res - 2u);

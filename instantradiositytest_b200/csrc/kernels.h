@@ -5,6 +5,19 @@
 #include "../../include/irt.h"
 #include "workload.h"
 
+namespace irtd {
+// The reference's filtered variant of sample_field (src/renderer.rs:277-286,
+// chosen there whenever the adapter can filter R32Float textures): one
+// hardware-linear fetch of the atlas at the normalised coordinate
+// (origin + q + .5) / dims, clamp-to-edge, instead of 8 texel loads and f32
+// weights.  linear == 0 selects the point-sampled trilinear of
+// common.wgsl:31-38.
+struct FieldFilter {
+    cudaTextureObject_t linear;  // the atlas: normalised coordinates, linear filter, clamp
+    float dims[3];               // atlas extent in texels
+};
+}  // namespace irtd
+
 // Lighting stages: 0..7 are the reference entry points in schedule order
 // (candidates_direct, candidates_indirect, temporal_direct, temporal_indirect,
 // spatial_direct, spatial_indirect, resolve_direct, resolve_indirect).
@@ -32,6 +45,7 @@ struct LightingLaunch {
     cudaTextureObject_t atlas;
     int sdf_f16;
     const void* sdf_cells;  // corner cells of the field meshes (dev_sdf.cuh), or null
+    irtd::FieldFilter field_filter;
     uint32_t* error;
     const irt_vpl* cur_vpls;
     const irt_vpl* prev_vpls;
@@ -62,6 +76,7 @@ struct MarchLaunch {
     cudaTextureObject_t atlas;
     int sdf_f16;
     const void* sdf_cells;  // corner cells of the field meshes (dev_sdf.cuh), or null
+    irtd::FieldFilter field_filter;
     uint32_t* error;
     const float4* march_scene;  // compact nodes + objects (irt_march_scene_bytes)
     // Leaf-order cache: a kGridRes^3 grid over the root box; per cell the
@@ -92,6 +107,7 @@ struct LeafCacheLaunch {
     cudaTextureObject_t atlas;
     int sdf_f16;
     const void* sdf_cells;  // corner cells of the field meshes (dev_sdf.cuh), or null
+    irtd::FieldFilter field_filter;
     double grid_org_d[3], grid_size_d[3];
     float* corners;             // (kGridRes+1)^3 * n floats, or null: box bounds only
     uint32_t* cells;            // kGridRes^3 * kCellWords words
@@ -141,6 +157,13 @@ cudaError_t irt_launch_lighting(const LightingLaunch& L, int stage, cudaStream_t
 // (res-1)^3) of `out` from the atlas tile at `origin` (DevScene::sdf_cells).
 cudaError_t irt_pack_sdf_cells(cudaTextureObject_t atlas, int f16, const uint32_t origin[3], uint32_t res,
                                uint64_t base, void* out, cudaStream_t st);
+// sample_field of the mesh `row` (its device row values: hi[3] = first
+// corner cell) at n grid-space points q (3 floats each); out: n floats.
+namespace irtd {
+struct DevScene;
+}
+cudaError_t irt_launch_sample_field(const irtd::DevScene& sc, const irt_mesh& row, const float* q, uint32_t n,
+                                    float* out, cudaStream_t st);
 
 // ------------------------------------------------------------------ batched views
 // One launch per pass over the views of a batch.  `table` is a device array
@@ -187,6 +210,7 @@ struct alignas(16) MarchGroup {
     cudaTextureObject_t atlas;
     int sdf_f16;
     const void* sdf_cells;  // corner cells of the field meshes (dev_sdf.cuh), or null
+    irtd::FieldFilter field_filter;
     uint32_t* error;
     const float4* march_scene;
     uint32_t scene_vec4;

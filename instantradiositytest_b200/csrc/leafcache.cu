@@ -137,6 +137,7 @@ cudaError_t irt_launch_leaf_cache(const LeafCacheLaunch& L, cudaStream_t st) {
     sc.atlas = L.atlas;
     sc.sdf_f16 = L.sdf_f16;
     sc.sdf_cells = L.sdf_cells;
+    sc.filter = L.field_filter;
     const MObj* objs = reinterpret_cast<const MObj*>(L.march_scene + 2 * (2 * L.n - 1));
     const MNode* nodes = reinterpret_cast<const MNode*>(L.march_scene);
     const int use_corners = L.corners != nullptr;

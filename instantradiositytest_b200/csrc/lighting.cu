@@ -610,6 +610,7 @@ static LightArgs<G> make_args(const LightingLaunch& L) {
     a.sc.atlas = L.atlas;
     a.sc.sdf_f16 = L.sdf_f16;
     a.sc.sdf_cells = L.sdf_cells;
+    a.sc.filter = L.field_filter;
     a.sc.error = L.error;
     a.cur = L.cur_vpls;
     a.prev = L.prev_vpls;

@@ -25,6 +25,8 @@
 // approximate division and square root for the default fast march.
 #include <cuda_runtime.h>
 
+#include <cstdlib>
+
 #include "dev_sdf.cuh"
 #include "kernels.h"
 
@@ -206,6 +208,192 @@ __global__ void __launch_bounds__(128, 8) march_kernel(const __grid_constant__ i
     }
 }
 
+// The march as one flattened loop: every iteration each lane evaluates at
+// most one object, the next candidate of its current distance query — the
+// hint object first (the previous closest, as scene_distance seeds it), then
+// the leaf-order cache entries of the query point's cell that survive the
+// walk's pruning tests, then (rarely) every leaf.  A lane whose query has no
+// candidate left completes it (the march step of sdf.wgsl:61-81), starts its
+// ray's next query, or takes a new ray, and finds that query's first
+// candidate within the same iteration.  Candidate order and pruning per
+// query are exactly scene_distance_cached's, so results are unchanged; the
+// object evaluations of lanes at different stages of their queries (a hint,
+// a second leaf, the first leaf of a new ray) issue together instead of in
+// separate divergent sections.
+struct Query {
+    V3 p;
+    float best;
+    uint32_t closest, hint;
+    int32_t cur;          // next candidate: -1 hint, 0..7 cache entries, 8 after them, >= kAll all leaves
+    const uint32_t* cw;   // the point's cache cell, or null outside the grid
+};
+constexpr int32_t kAfterEntries = (int32_t)kCellEntries;
+constexpr int32_t kAll = 16;
+constexpr int32_t kQueryDone = 0x7fffffff;
+
+__device__ __forceinline__ void query_begin(Query& qy, const Grid& g, V3 p, uint32_t hint, uint32_t n) {
+    qy.p = p;
+    qy.best = 1e20f;
+    qy.closest = hint;
+    qy.hint = hint;
+    const float fx = (p.x - g.ox) * g.ix, fy = (p.y - g.oy) * g.iy, fz = (p.z - g.oz) * g.iz;
+    const float G = (float)kGridRes;
+    const bool inside = fx >= 0.f && fy >= 0.f && fz >= 0.f && fx < G && fy < G && fz < G;
+    qy.cw = nullptr;
+    if (inside) {
+        const uint32_t cell = ((uint32_t)fz * kGridRes + (uint32_t)fy) * kGridRes + (uint32_t)fx;
+        qy.cw = reinterpret_cast<const uint32_t*>(g.cells + (size_t)cell * (kCellWords / 4));
+    }
+    qy.cur = hint < n ? -1 : (inside ? 0 : kAll);
+}
+
+// The walk's pruning test of leaf `oid`'s box against the best so far.
+__device__ __forceinline__ bool leaf_may_hold_best(const MNode* nodes, const MObj* objs, V3 p, uint32_t oid,
+                                                   float best) {
+    const uint32_t leaf = __float_as_uint(objs[oid].meta.w);
+    const float4 a = nodes[leaf].a, b = nodes[leaf].b;
+    V3 delta = vmax(vmax(V3{a.x, a.y, a.z} - p, p - V3{b.x, b.y, b.z}), V3{0.f, 0.f, 0.f});
+    V3 lb = delta * .9998f;
+    float bb = wmax(best, 0.f);
+    return !(dot(lb, lb) > bb * bb);
+}
+
+// Next object to evaluate for the query, or kNone when the query is complete.
+__device__ __forceinline__ uint32_t query_next(Query& qy, const MNode* nodes, const MObj* objs, uint32_t n) {
+    for (;;) {
+        const int32_t c = qy.cur;
+        if (c < 0) {  // the hint, unconditionally
+            qy.cur = qy.cw ? 0 : kAll;
+            return qy.hint;
+        }
+        if (c < kAfterEntries) {
+            const uint32_t oid = (__ldg(qy.cw + (c >> 1)) >> ((c & 1) * 16)) & 0xffffu;
+            if (__uint_as_float(__ldg(qy.cw + 4 + c)) > wmax(qy.best, 0.f) || oid == 0xffffu) {
+                qy.cur = kQueryDone;
+                return kNone;
+            }
+            qy.cur = c + 1;
+            if (oid != qy.hint && leaf_may_hold_best(nodes, objs, qy.p, oid, qy.best)) return oid;
+            continue;
+        }
+        if (c == kAfterEntries) {  // every cached entry fits: the ones left out may too
+            qy.cur = __uint_as_float(__ldg(qy.cw + 12)) <= wmax(qy.best, 0.f) ? kAll : kQueryDone;
+            continue;
+        }
+        if (c < kAll + (int32_t)n) {
+            const uint32_t oid = (uint32_t)(c - kAll);
+            qy.cur = c + 1;
+            if (oid != qy.hint && leaf_may_hold_best(nodes, objs, qy.p, oid, qy.best)) return oid;
+            continue;
+        }
+        return kNone;
+    }
+}
+
+__global__ void __launch_bounds__(128, 8) march_flat_kernel(const __grid_constant__ irt_frame f, const DevScene sc,
+                                                         const float4* __restrict__ march_scene, uint32_t scene_vec4,
+                                                         const Grid grid, const RayRecord* __restrict__ rays,
+                                                         uint32_t* counters, float* __restrict__ vis) {
+    extern __shared__ float4 smem[];
+    for (uint32_t i = threadIdx.x; i < scene_vec4; i += blockDim.x) smem[i] = __ldg(march_scene + i);
+    __syncthreads();
+    const uint32_t n_obj = f.counts[3];
+    const MNode* nodes = reinterpret_cast<const MNode*>(smem);
+    const MObj* objs = reinterpret_cast<const MObj*>(smem + 2 * (2 * n_obj - 1));
+
+    const uint32_t front = *(volatile uint32_t*)&counters[0];
+    const uint32_t n_rays = front + *(volatile uint32_t*)&counters[2];
+    const uint32_t cap = 2u * f.size[0] * f.size[1];
+    const unsigned full = 0xffffffffu;
+    const int lane = threadIdx.x & 31;
+    const float eps = f.sdf[1];
+    const uint32_t max_steps = to_u32(f.sdf[0]);
+
+    bool active = false;
+    bool exhausted = false;  // warp-uniform: the queue has no rays left
+    uint32_t phase = kClear, ridx = 0;
+    MarchState m;
+    m.closest = kNone;
+    m.origin = V3{0.f, 0.f, 0.f};
+    m.dir = V3{0.f, 0.f, 0.f};
+    m.t = m.limit = 0.f;
+    m.result = 1.f;
+    m.previous = 1e20f;
+    m.step = 0;
+    Query qy;
+    qy.cur = kQueryDone;
+    for (;;) {
+        if (!exhausted) {
+            unsigned need = __ballot_sync(full, !active);
+            if (need) {
+                int leader = __ffs(need) - 1;
+                uint32_t cnt = (uint32_t)__popc(need);
+                uint32_t base = 0;
+                if (lane == leader) base = atomicAdd(&counters[1], cnt);
+                base = __shfl_sync(full, base, leader);
+                if (base + cnt >= n_rays) exhausted = true;
+                if (!active) {
+                    uint32_t idx = base + (uint32_t)__popc(need & ((1u << lane) - 1u));
+                    if (idx < n_rays) {
+                        ridx = ray_slot(idx, front, cap);
+                        const float4* r = reinterpret_cast<const float4*>(rays + ridx);
+                        float4 a = __ldg(r), b = __ldg(r + 1);
+                        m.origin = V3{a.x, a.y, a.z};
+                        m.dir = V3{b.x, b.y, b.z};
+                        phase = kClear;
+                        active = true;
+                        query_begin(qy, grid, m.origin, kNone, n_obj);  // the clearance query
+                    }
+                }
+            }
+        }
+        if (!__any_sync(full, active)) break;
+        if (!active) continue;
+
+        uint32_t oid = query_next(qy, nodes, objs, n_obj);
+        while (oid == kNone) {
+            // The query is complete: the march step it feeds (as march_kernel).
+            const float4* rec = reinterpret_cast<const float4*>(rays + ridx);
+            const float voxel = (phase != kMarch && qy.closest < n_obj) ? objs[qy.closest].meta.y : eps;
+            float out = -1.f;
+            if (phase == kClear) {
+                m.closest = qy.closest;
+                m.origin = m.origin + m.dir * clearance_epsilon(eps, voxel);
+                const V3 endn = xyz(__ldg(rec + 3));
+                if (dot(endn, endn) > .5f) {
+                    phase = kEndpoint;
+                } else {
+                    phase = kMarch;
+                    out = march_begin(m, xyz(__ldg(rec + 2)), eps, max_steps);
+                }
+            } else if (phase == kEndpoint) {
+                phase = kMarch;
+                const V3 target = xyz(__ldg(rec + 2)), endn = xyz(__ldg(rec + 3));
+                out = march_begin(m, target + endn * clearance_epsilon(eps, voxel), eps, max_steps);
+            } else {
+                m.closest = qy.closest;
+                out = march_after(m, qy.best, eps, f.sdf[2], max_steps);
+            }
+            if (out >= 0.f) {
+                vis[__float_as_uint(__ldg(rec).w)] = out;
+                active = false;
+                break;
+            }
+            // the ray's next query
+            const V3 q = phase == kEndpoint ? xyz(__ldg(rec + 2)) : march_point(m);
+            query_begin(qy, grid, q, phase == kMarch ? m.closest : kNone, n_obj);
+            oid = query_next(qy, nodes, objs, n_obj);
+        }
+        if (oid != kNone) {
+            const float d = object_distance_rec(sc, qy.p, objs[oid]);
+            if (oid == qy.hint || d < qy.best) {  // the hint sets the best unconditionally
+                qy.best = d;
+                qy.closest = oid;
+            }
+        }
+    }
+}
+
 // Batched march: for each scene group the CTA stages the group record and
 // its compact scene in shared memory, then its warps consume the group's ray
 // queues (one per view) in order with the same per-lane state machine; a
@@ -237,6 +425,7 @@ __global__ void __launch_bounds__(128, 8) march_batched_kernel(const MarchGroup*
         sc.atlas = G.atlas;
         sc.sdf_f16 = G.sdf_f16;
         sc.sdf_cells = G.sdf_cells;
+        sc.filter = G.field_filter;
         sc.error = G.error;
         Grid grid;
         grid.cells = G.cells;
@@ -374,6 +563,7 @@ cudaError_t IRT_MARCH_LAUNCH(const MarchLaunch& M, cudaStream_t st) {
     sc.atlas = M.atlas;
     sc.sdf_f16 = M.sdf_f16;
     sc.sdf_cells = M.sdf_cells;
+    sc.filter = M.field_filter;
     sc.error = M.error;
     Grid g;
     g.cells = M.cells;
@@ -383,6 +573,25 @@ cudaError_t IRT_MARCH_LAUNCH(const MarchLaunch& M, cudaStream_t st) {
     g.ix = M.grid_inv[0];
     g.iy = M.grid_inv[1];
     g.iz = M.grid_inv[2];
+    static const bool flat = getenv("IRT_MARCH_FLAT") && getenv("IRT_MARCH_FLAT")[0] == '1';
+    if (flat) {
+        thread_local int flat_device = -1;
+        thread_local uint32_t flat_smem = 0;
+        thread_local int flat_blocks = 0;
+        if (smem != flat_smem || device != flat_device) {
+            flat_device = device;
+            cudaError_t e = cudaFuncSetAttribute(march_flat_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                                 (int)smem);
+            if (e != cudaSuccess) return e;
+            e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&flat_blocks, march_flat_kernel, 128, smem);
+            if (e != cudaSuccess) return e;
+            if (flat_blocks < 1) return cudaErrorInvalidConfiguration;
+            flat_smem = smem;
+        }
+        march_flat_kernel<<<M.num_sms * flat_blocks, 128, smem, st>>>(*M.frame, sc, M.march_scene, smem / 16, g,
+                                                                       M.rays, M.ray_counters, M.vis);
+        return cudaGetLastError();
+    }
     march_kernel<<<M.num_sms * blocks_per_sm, 128, smem, st>>>(*M.frame, sc, M.march_scene, smem / 16, g, M.rays,
                                                                 M.ray_counters, M.vis);
     return cudaGetLastError();

@@ -7,9 +7,19 @@
 #include <cuda_fp16.h>
 #include <cuda_runtime.h>
 
+#include "dev_sdf.cuh"
 #include "kernels.h"
 
 namespace {
+
+// sample_field of one mesh at n grid-space points with the kernels' own
+// sampler (the point-sampled trilinear of the IEEE build, or the hardware
+// linear fetch).
+__global__ void sample_points_kernel(const irtd::DevScene sc, const irtd::DMesh m, const float* __restrict__ q,
+                                     uint32_t n, float* __restrict__ out) {
+    for (uint32_t i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x)
+        out[i] = irtd::sample_field(sc, m, irtd::V3{q[3 * i], q[3 * i + 1], q[3 * i + 2]});
+}
 
 __global__ void pack_cells_kernel(cudaTextureObject_t atlas, int f16, uint3 origin, uint32_t res, uint64_t base,
                                   void* out) {
@@ -40,6 +50,22 @@ __global__ void pack_cells_kernel(cudaTextureObject_t atlas, int f16, uint3 orig
 }
 
 }  // namespace
+
+cudaError_t irt_launch_sample_field(const irtd::DevScene& sc, const irt_mesh& row, const float* q, uint32_t n,
+                                    float* out, cudaStream_t st) {
+    irtd::DMesh m;
+    m.lo = make_float4(row.lo[0], row.lo[1], row.lo[2], row.lo[3]);
+    m.hi = make_float4(row.hi[0], row.hi[1], row.hi[2], row.hi[3]);
+    m.field = make_uint4(row.field[0], row.field[1], row.field[2], row.field[3]);
+    m.grid = make_float4(row.grid[0], row.grid[1], row.grid[2], row.grid[3]);
+    m.glo = make_float4(row.geometry_lo[0], row.geometry_lo[1], row.geometry_lo[2], row.geometry_lo[3]);
+    m.ghi = make_float4(row.geometry_hi[0], row.geometry_hi[1], row.geometry_hi[2], row.geometry_hi[3]);
+    m.sphere = make_float4(row.enclosing_sphere[0], row.enclosing_sphere[1], row.enclosing_sphere[2],
+                           row.enclosing_sphere[3]);
+    const uint32_t blocks = (n + 255) / 256 < 148u * 8u ? (n + 255) / 256 : 148u * 8u;
+    sample_points_kernel<<<blocks, 256, 0, st>>>(sc, m, q, n, out);
+    return cudaGetLastError();
+}
 
 cudaError_t irt_pack_sdf_cells(cudaTextureObject_t atlas, int f16, const uint32_t origin[3], uint32_t res,
                                uint64_t base, void* out, cudaStream_t st) {

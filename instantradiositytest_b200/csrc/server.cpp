@@ -60,7 +60,7 @@ struct Active {
     uint64_t bytes = 0;
     uint32_t W = 0, H = 0, vpl_count = 0;
     uint32_t next_frame = 0;
-    double admitted = 0;
+    double admitted = 0, last_done = 0;
     std::vector<irt_object> objects;
     std::vector<irt_node> nodes;
     std::vector<irt_light> lights;
@@ -153,6 +153,7 @@ extern "C" void irt_server_destroy(irt_server* s) {
 
 extern "C" irt_status irt_server_submit(irt_server* s, const irt_request* r) {
     if (!s || !r || !r->workload || r->frames == 0 || !(r->arrival_s >= 0.0)) return IRT_E_INVALID;
+    if (r->times) r->times[0] = r->times[1] = r->times[2] = -1.0;
     // keep the queue ordered by arrival (stable for equal times)
     auto it = std::upper_bound(s->queue.begin(), s->queue.end(), *r,
                                [](const irt_request& a, const irt_request& b) { return a.arrival_s < b.arrival_s; });
@@ -307,6 +308,7 @@ extern "C" irt_status irt_server_run(irt_server* s, irt_server_stats* stats) {
                 latency.push_back((float)((done - fl.due) * 1000.0));
                 frame_ms.push_back(ms_frame);
                 last_done = std::max(last_done, done);
+                a->last_done = std::max(a->last_done, done);
                 frames++;
                 pixel_frames += (double)a->W * a->H;
                 if (fl.capture) std::memcpy(a->req.capture, a->staging, a->capture_bytes);
@@ -319,6 +321,11 @@ extern "C" irt_status irt_server_run(irt_server* s, irt_server_stats* stats) {
                 // All of the session's work has completed: read its error
                 // word on the idle control stream, not behind other sessions.
                 if (irt_session_check(a->session, s->control) != IRT_OK) rc = IRT_E_DEVICE;
+                if (a->req.times) {
+                    a->req.times[0] = a->admitted;
+                    a->req.times[1] = a->last_done;
+                    a->req.times[2] = seconds_since(t0);
+                }
                 admitted_bytes -= a->bytes;
                 release(a);
                 active.erase(active.begin() + (long)i);

@@ -5,16 +5,18 @@
 // thread must not stall on the device-wide synchronisation an allocation can
 // imply, or an application that reserves all device memory up front under
 // its own allocator and budget.  This entry point serves them: the caller
-// passes every input and output, and the two ping-pong images the filter
-// needs between its passes live in a fixed array of this library's device
-// memory instead of a session.
+// passes every input and output, and what the filter needs in between — the
+// per-pixel positions and edge-stopping features of the frame and the two
+// ping-pong images of the a-trous passes — lives in a fixed array of this
+// library's device memory instead of a session.
 //
-// The array (kNoAllocMaxPixels f32x4 texels x 2 = 8 MiB) is a file-scope
+// The array (kNoAllocMaxPixels x 5 f32x4 texels = 20 MiB) is a file-scope
 // __device__ variable: every GPU that loads the library holds it until the
 // process exits.  Frames above kNoAllocMaxPixels pixels are rejected.  All
-// calls share the array and it keeps the last call's contents, so calls that
-// overlap on the GPU (on different streams, or from different host threads
-// without ordering) race on it.
+// calls share the array and it keeps the last call's contents (each call
+// rewrites every texel it reads before reading it), so calls that overlap on
+// the GPU (on different streams, or from different host threads without
+// ordering) race on it.
 #include <cuda_runtime.h>
 
 #include <cstdio>
@@ -27,12 +29,18 @@ namespace {
 constexpr uint32_t kNoAllocMaxPixels = 512u * 512u;
 constexpr int kMaxDevices = 64;
 
-// Two ping-pong images of up to kNoAllocMaxPixels texels (f32x4; f16x4
-// images use the first half of each).
-static __device__ __align__(256) float4 g_svgf_scratch[2][kNoAllocMaxPixels];
+// Per pixel: [0] ping and [1] pong a-trous images (f32x4; f16x4 images use
+// the first half of each), [2] world position + SVGF pixel scale, [3..4]
+// edge-stopping feature records (two f32x4 per pixel, decoded G-buffer
+// formats only).
+static __device__ __align__(256) float4 g_svgf_scratch[5][kNoAllocMaxPixels];
 
-// Device address of g_svgf_scratch per device ordinal.  In host code the
-// symbol itself is only a host-side stand-in, never a device address.
+// Device address of g_svgf_scratch per device ordinal, looked up on the first
+// call on that device.  In host code the symbol itself is only a host-side
+// stand-in, never a device address.  The cached address belongs to the
+// device's primary context: a caller that resets the device
+// (cudaDeviceReset) while the library stays loaded must not call this entry
+// point again in that process.
 std::mutex g_mu;
 float4* g_scratch_ptr[kMaxDevices] = {};
 
@@ -43,10 +51,10 @@ void fail(char* err, size_t err_len, const char* msg) {
 }  // namespace
 
 extern "C" irt_status irt_svgf_spatial_noalloc(const irt_frame* frame, const irt_gbuffer* gbuffer,
-                                               int32_t radiance_format, uint32_t iterations,
-                                               const void* temporal_radiance, const float* moments,
-                                               void* filtered_out, void* feedback_out, void* stream, char* err,
-                                               size_t err_len) {
+                                               int32_t radiance_format, int32_t moments_format,
+                                               uint32_t iterations, const void* temporal_radiance,
+                                               const void* moments, void* filtered_out, void* feedback_out,
+                                               void* stream, char* err, size_t err_len) {
     if (err && err_len) err[0] = 0;
     if (!frame || !gbuffer || !temporal_radiance || !moments || !filtered_out) {
         fail(err, err_len, "null argument");
@@ -57,11 +65,21 @@ extern "C" irt_status irt_svgf_spatial_noalloc(const irt_frame* frame, const irt
         fail(err, err_len, "frame exceeds the allocation-free filter's maximum of 262144 pixels (512x512)");
         return IRT_E_INVALID;
     }
-    if (iterations == 0 || iterations > 5 ||
-        (radiance_format != IRT_RADIANCE_F32 && radiance_format != IRT_RADIANCE_F16) ||
-        gbuffer->format < IRT_GBUFFER_F32 || gbuffer->format > IRT_GBUFFER_PACKED || !gbuffer->depth ||
+    if (iterations == 0 || iterations > 5) {
+        fail(err, err_len, "svgf iterations must be 1..5");
+        return IRT_E_INVALID;
+    }
+    if (radiance_format != IRT_RADIANCE_F32 && radiance_format != IRT_RADIANCE_F16) {
+        fail(err, err_len, "unknown radiance format");
+        return IRT_E_INVALID;
+    }
+    if (moments_format != IRT_MOMENTS_F32 && moments_format != IRT_MOMENTS_F16) {
+        fail(err, err_len, "unknown moments format");
+        return IRT_E_INVALID;
+    }
+    if (gbuffer->format < IRT_GBUFFER_F32 || gbuffer->format > IRT_GBUFFER_PACKED || !gbuffer->depth ||
         !gbuffer->normal || !gbuffer->color || !gbuffer->params || !gbuffer->motion) {
-        fail(err, err_len, "invalid iterations, radiance format or G-buffer");
+        fail(err, err_len, "invalid G-buffer format or planes");
         return IRT_E_INVALID;
     }
     int dev = 0;
@@ -86,16 +104,28 @@ extern "C" irt_status irt_svgf_spatial_noalloc(const irt_frame* frame, const irt
     }
     float4* ping = scratch;
     float4* pong = scratch + kNoAllocMaxPixels;
+    float4* guide = scratch + 2 * kNoAllocMaxPixels;
+    float4* feat = scratch + 3 * kNoAllocMaxPixels;
     cudaStream_t st = static_cast<cudaStream_t>(stream);
     SvgfLaunch L{};
     L.frame = frame;
     L.gbuffer = *gbuffer;
     L.radiance_f16 = radiance_format == IRT_RADIANCE_F16;
+    L.moments_f16 = moments_format == IRT_MOMENTS_F16;
+    // The frame's per-pixel positions (and, for the F16 and packed G-buffers,
+    // decoded edge-stopping features), written by the same kernels a session
+    // runs before its SVGF passes, so the results equal a session's.
+    L.out = guide;
+    L.out2 = feat;
+    cudaError_t e = irt_launch_svgf(L, gbuffer->format == IRT_GBUFFER_F32 ? 3 : 6, st);
+    L.guide = guide;
+    L.feat = feat;
     // svgf_variance (svgf.wgsl:77-89): temporal radiance + moments -> ping.
     L.in = temporal_radiance;
     L.moments_in = moments;
     L.out = ping;
-    cudaError_t e = irt_launch_svgf(L, 1, st);
+    L.out2 = nullptr;
+    if (e == cudaSuccess) e = irt_launch_svgf(L, 1, st);
     // svgf_atrous x iterations (svgf.wgsl:91-110), the same buffer order as a
     // session: iteration 0 also gives the feedback image, the last writes
     // filtered_out, the others alternate between pong and ping.

@@ -74,6 +74,22 @@ class Scene:
                                      len(lights), stream if stream is not None else stream_handle()),
                 self.ctx.handle, "scene update")
 
+    def set_field_filter(self, field_filter: int):
+        """L.FIELD_POINT or L.FIELD_LINEAR (the reference's hardware-filtered
+        sample_field), from the next update on."""
+        L.check(lib.irt_scene_set_field_filter(self.handle, field_filter), self.ctx.handle, "field filter")
+
+    def sample_field(self, mesh: int, q: np.ndarray, field_filter: int = L.FIELD_POINT) -> np.ndarray:
+        """sample_field of field mesh `mesh` at grid-space points q [n, 3]
+        with the kernels' sampler; returns float32 [n]."""
+        qd = torch.from_numpy(np.ascontiguousarray(q, np.float32).reshape(-1)).cuda()
+        n = qd.numel() // 3
+        out = torch.empty(n, dtype=torch.float32, device="cuda")
+        L.check(lib.irt_scene_sample_field(self.handle, field_filter, mesh, C.c_void_p(qd.data_ptr()), n,
+                                           C.c_void_p(out.data_ptr()), stream_handle()), self.ctx.handle,
+                "sample field")
+        return out.cpu().numpy()
+
     def close(self):
         if self.handle:
             lib.irt_scene_destroy(self.handle)

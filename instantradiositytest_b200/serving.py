@@ -24,22 +24,29 @@ class Server:
         self.handle = h
         self._keep = []
 
-    def submit(self, request_id: int, arrival_s: float, frames: int, workload, capture_frame: int | None = None):
+    def submit(self, request_id: int, arrival_s: float, frames: int, workload, capture_frame: int | None = None,
+               times: np.ndarray | None = None):
         """Queues a render session over `workload`; with capture_frame, returns
-        the host array that receives that frame's filtered image."""
+        the host array that receives that frame's filtered image.  times: a
+        float64 array of 3 that the run fills with the session's admission,
+        last-frame-done and retirement times (seconds after the run starts)."""
         out = None
         cap = None
         if capture_frame is not None:
             texel = 8 if self.desc.radiance_format == L.RADIANCE_F16 else 16
             out = np.zeros(workload.width * workload.height * texel, np.uint8)
             cap = C.c_void_p(out.ctypes.data)
-        r = L.Request(request_id, arrival_s, frames, workload.handle, capture_frame or 0, cap)
+        tp = None
+        if times is not None:
+            assert times.dtype == np.float64 and times.size >= 3 and times.flags["C_CONTIGUOUS"]
+            tp = times.ctypes.data_as(C.POINTER(C.c_double))
+        r = L.Request(request_id, arrival_s, frames, workload.handle, capture_frame or 0, cap, tp)
         L.check(lib.irt_server_submit(self.handle, C.byref(r)), self.ctx.handle, "server submit")
-        self._keep.append((workload, out))
+        self._keep.append((workload, out, times))
         return out
 
     def request_bytes(self, workload, frames: int = 1) -> int:
-        r = L.Request(0, 0.0, frames, workload.handle, 0, None)
+        r = L.Request(0, 0.0, frames, workload.handle, 0, None, None)
         return int(lib.irt_server_request_bytes(self.handle, C.byref(r)))
 
     def run(self) -> dict:

@@ -79,6 +79,9 @@ def _load():
         lib.oracle_normalization.argtypes = [P]
         lib.oracle_quilez_step.restype = C.c_float
         lib.oracle_quilez_step.argtypes = [C.c_float] * 5
+        lib.oracle_set_field_filter.argtypes = [P, C.c_int]
+        lib.oracle_sample_field.restype = C.c_float
+        lib.oracle_sample_field.argtypes = [P, P, C.POINTER(C.c_uint32), C.POINTER(C.c_float), C.c_int]
         lib.oracle_mesh_distance.restype = C.c_float
         lib.oracle_mesh_distance.argtypes = [P, P, C.POINTER(C.c_uint32), C.POINTER(C.c_float)]
         _lib = lib
@@ -87,6 +90,17 @@ def _load():
 
 def lib():
     return _load()
+
+
+def sample_field(mesh: np.ndarray, atlas_f32: np.ndarray, q, linear: int) -> float:
+    """sample_field of one mesh row (MESH_DTYPE record) at grid-space point q
+    over an f32 atlas [z, y, x]."""
+    lib = _load()
+    a = np.ascontiguousarray(atlas_f32, np.float32)
+    m = np.ascontiguousarray(mesh)
+    dims = (C.c_uint32 * 3)(a.shape[2], a.shape[1], a.shape[0])
+    qq = (C.c_float * 3)(*[float(v) for v in q])
+    return float(lib.oracle_sample_field(_p(m), _p(a), dims, qq, int(linear)))
 
 
 def f16_bits(v: float) -> int:
@@ -137,6 +151,11 @@ class Oracle:
             self.close()
         except Exception:
             pass
+
+    def set_field_filter(self, linear: int):
+        """0: point-sampled sample_field (common.wgsl:31-38); 1: the
+        reference's hardware-filtered variant (src/renderer.rs:277-286)."""
+        self.lib.oracle_set_field_filter(self.h_, int(linear))
 
     def set_rows(self, row0=0, row1=0xFFFFFFFF):
         """Evaluate only rows [row0, row1) (a timing band of a large frame)."""

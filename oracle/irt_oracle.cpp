@@ -146,6 +146,7 @@ struct Scene {
     const irt_light* lights;
     const float* atlas;  // dequantised texels, x fastest
     uint32_t dims[3];
+    int field_linear = 0;  // 1: the reference's hardware-filtered sample_field
 };
 
 struct GBuffer {  // F32 layout
@@ -402,8 +403,45 @@ struct Path {
     T texel(uint32_t x, uint32_t y, uint32_t z) const {
         return (T)sc.atlas[((size_t)z * sc.dims[1] + y) * sc.dims[0] + x];
     }
+    // The reference's filtered variant of sample_field (src/renderer.rs:
+    // 277-286): textureSampleLevel(fields, field_sampler,
+    // (vec3(origin) + q + .5) / vec3(dims), 0.) through a clamp-to-edge
+    // linear sampler.  The filter is restated from the linear-filtering
+    // formula of the CUDA C++ Programming Guide ("Texture Fetching"
+    // appendix), which the device sampler implements: at the unnormalised
+    // coordinate x = u * N, x_B = x - 0.5, i = floor(x_B) and
+    // alpha = frac(x_B) held in 9-bit fixed point with 8 fractional bits
+    // (here rounded to the nearest 1/256), and the value is the sum over the
+    // 8 texels of (1 - alpha or alpha) products per axis, clamped to the
+    // atlas edge.  Weighted in the same z, y, x order as sample_field.
+    T linear_field(const uint32_t origin[3], V3<T> q) const {
+        const T qa[3] = {q.x, q.y, q.z};
+        int64_t i0[3];
+        T alpha[3];
+        for (int a = 0; a < 3; a++) {
+            const T u = (((T)origin[a] + qa[a]) + (T).5) / (T)sc.dims[a];
+            const double xb = (double)u * (double)sc.dims[a] - 0.5;
+            const double fl = std::floor(xb);
+            i0[a] = (int64_t)fl;
+            alpha[a] = (T)(std::floor((xb - fl) * 256.0 + 0.5) / 256.0);
+        }
+        auto at = [&](int a, int64_t i) {
+            return (uint32_t)std::min<int64_t>(std::max<int64_t>(i, 0), (int64_t)sc.dims[a] - 1);
+        };
+        T value = 0;
+        for (uint32_t z = 0; z < 2; z++)
+            for (uint32_t y = 0; y < 2; y++)
+                for (uint32_t x = 0; x < 2; x++) {
+                    T wx = x == 1 ? alpha[0] : (T)1 - alpha[0];
+                    T wy = y == 1 ? alpha[1] : (T)1 - alpha[1];
+                    T wz = z == 1 ? alpha[2] : (T)1 - alpha[2];
+                    value += texel(at(0, i0[0] + x), at(1, i0[1] + y), at(2, i0[2] + z)) * wx * wy * wz;
+                }
+        return value;
+    }
     // common.wgsl:31-38
     T sample_field(const uint32_t origin[3], V3<T> q, uint32_t res) const {
+        if (sc.field_linear) return linear_field(origin, q);
         uint32_t cx = std::min(to_u32(std::floor(q.x)), res - 2u);
         uint32_t cy = std::min(to_u32(std::floor(q.y)), res - 2u);
         uint32_t cz = std::min(to_u32(std::floor(q.z)), res - 2u);
@@ -537,6 +575,7 @@ struct State {
     uint32_t W = 0, H = 0, vpl_count = 0, max_history = 0;
     int precision = 0;      // 0 = FP32, 1 = FP64
     int radiance_f16 = 0;   // Rgba16Float storage points
+    int field_filter = 0;   // 1: hardware-filtered sample_field (src/renderer.rs:277-286)
     int threads = 0;
     // Rows [row0, row1) that the passes evaluate (the whole image unless a
     // timing sample restricts it to a band).
@@ -1079,6 +1118,7 @@ int oracle_lighting(void* s, const irt_frame* f, const oracle_scene* scene, cons
     if (f->size[0] != st->W || f->size[1] != st->H || f->counts[1] != st->vpl_count) return -1;
     if (f->counts[3] == 0u) return -1;
     Scene sc = to_scene(scene);
+    sc.field_linear = st->field_filter;
     GBuffer g = to_gbuffer(gb);
     if (st->precision == 1)
         lighting_passes<double>(*st, *f, sc, g, cur, prev, first_pass, last_pass);
@@ -1212,6 +1252,24 @@ float oracle_quilez_step(float result, float h, float previous, float t, float k
     float d = std::sqrt(fmax_(h * h - y * y, 0.f));
     if (t > y) result = fmin_(result, k * d / (t - y));
     return result;
+}
+
+// Field sampler of the session's march: 0 point-sampled trilinear
+// (common.wgsl:31-38), 1 the reference's filtered variant.
+void oracle_set_field_filter(void* s, int filter) { static_cast<State*>(s)->field_filter = filter; }
+
+// sample_field of one mesh at grid-space point q over an f32 atlas: the
+// point-sampled form or the filtered variant.
+float oracle_sample_field(const irt_mesh* mesh, const float* atlas, const uint32_t dims[3], const float q[3],
+                          int linear) {
+    Scene sc{};
+    sc.atlas = atlas;
+    for (int i = 0; i < 3; i++) sc.dims[i] = dims[i];
+    sc.field_linear = linear;
+    irt_frame f{};
+    GBuffer g{};
+    Path<float> path(f, sc, g, nullptr, nullptr, nullptr, nullptr);
+    return path.sample_field(mesh->field, ld3<float>(q), mesh->field[3]);
 }
 
 // mesh_distance (sdf.wgsl:5-33) of one mesh over an f32 atlas.

@@ -14,7 +14,7 @@ import torch
 
 from instantradiositytest_b200 import _lib as L
 from instantradiositytest_b200.runtime import FrameDriver
-from instantradiositytest_b200.workload import Workload, gbuffer_as_f32
+from instantradiositytest_b200.workload import Workload, alloc_gbuffer, gbuffer_as_f32
 from oracle import Oracle, OracleScene
 from oracle import binding as ob
 
@@ -69,9 +69,19 @@ def outputs(o: Oracle, index: int):
             "moments": o.image(ob.MOMENTS[index % 2])[..., :3]}
 
 
+def download_gbuffer(gt: dict, h: int, w: int, fmt: int) -> dict:
+    """Device G-buffer planes (uint8 tensors, as FrameDriver keeps them) ->
+    host planes of `fmt` with the shapes and dtypes of alloc_gbuffer."""
+    out = alloc_gbuffer(h, w, fmt)
+    for k, v in out.items():
+        v.reshape(-1).view(np.uint8)[:] = gt[k].cpu().numpy()
+    return out
+
+
 class Lockstep:
     def __init__(self, wl: Workload, gbuffer_format=L.GBUFFER_F32, radiance_format=L.RADIANCE_F32, fused=1,
-                 precision=0, moments_format=L.MOMENTS_F32, oracle_f16_storage=None, f64_witness=False):
+                 precision=0, moments_format=L.MOMENTS_F32, oracle_f16_storage=None, f64_witness=False,
+                 gpu_gbuffer=False, field_filter=L.FIELD_POINT, gpu_vpls=False):
         """precision 0: the oracle in f32 (the reference's arithmetic), 1: in
         f64.  oracle_f16_storage: round the oracle's radiance history to f16
         as the reference's Rgba16Float does (default: when the radiance
@@ -79,15 +89,26 @@ class Lockstep:
         storage from the same synced history, and report the error of the
         CUDA outputs (`f64_<output>`) and of the primary oracle
         (`floor_<output>`, the f32 arithmetic's own distance from f64)
-        against it."""
+        against it.  gpu_gbuffer: the G-buffer comes from the CUDA producer
+        (irt_gbuffer_render, as in the benchmark) and the oracle is given
+        the planes the device rendered; otherwise both get the CPU one.
+        field_filter: the SDF sampler of both sides (L.FIELD_LINEAR: the
+        reference's hardware-filtered sample_field, emulated by the oracle).
+        gpu_vpls: the VPL pools come from the CUDA generator
+        (irt_vpl_generate) and the oracle is given the pools it wrote."""
         self.wl = wl
         self.drv = FrameDriver(wl, gbuffer_format=gbuffer_format, radiance_format=radiance_format, fused=fused,
-                               keep_candidates=True, moments_format=moments_format)
+                               keep_candidates=True, moments_format=moments_format, gpu_gbuffer=gpu_gbuffer,
+                               gpu_vpls=gpu_vpls)
         if oracle_f16_storage is None:
             oracle_f16_storage = radiance_format == L.RADIANCE_F16
         args = (wl.width, wl.height, wl.settings.vpl_count, wl.settings.restir_max_history)
         self.orc = Oracle(*args, precision, oracle_f16_storage)
         self.witness = Oracle(*args, 1, False) if f64_witness else None
+        self.drv.scene.set_field_filter(field_filter)
+        for o in (self.orc, self.witness):
+            if o is not None:
+                o.set_field_filter(field_filter)
         self.fmt = gbuffer_format
         self.prev_vpls = None
         self.atlas = atlas_f32(wl)
@@ -101,6 +122,10 @@ class Lockstep:
                 sync_history(o, self.drv, index - 1)
         self.drv.step(index, debug, inputs=inputs)
         torch.cuda.synchronize()
+        if planes is None:  # the CUDA producer's planes, as the kernels read them
+            planes = download_gbuffer(self.drv.last[6], self.wl.height, self.wl.width, self.fmt)
+        if vpls is None:  # the CUDA generator's pool of this frame
+            vpls = self.drv.prev_vpls.cpu().numpy().view(L.VPL_DTYPE).copy()
         prev = self.prev_vpls if self.prev_vpls is not None else np.zeros_like(vpls)
         sc = OracleScene(obj, self.wl.meshes, nodes, lights, self.atlas)
         g = gbuffer_as_f32(planes, self.fmt)

@@ -1,0 +1,141 @@
+"""The SDF field samplers on the device against the oracle.
+
+The reference samples a mesh's SDF tile either with 8 texel loads and f32
+trilinear weights (sample_field, common.wgsl:31-38) or, whenever the adapter
+can filter R32Float textures, with one hardware-linear fetch through its
+clamp-to-edge field_sampler (src/renderer.rs:277-286, :736-739, :914-921,
+:1470-1471).  IRT_FIELD_LINEAR is that filtered variant on the CUDA texture
+path; the oracle restates the linear-filtering formula of the CUDA C++
+Programming Guide (9-bit fixed-point weights with 8 fractional bits).
+
+* point sampler: the kernels' sample_field against the oracle's;
+* linear sampler, weights: on an atlas whose texels hold their own x index,
+  the fetched value minus the base texel is the hardware's x weight, which
+  must equal the emulated fixed-point weight;
+* linear sampler, values: random points of the rooms' real fields;
+* the hot path in lockstep with the oracle, both on the filtered sampler.
+"""
+import numpy as np
+import pytest
+
+from instantradiositytest_b200 import _lib as L
+from instantradiositytest_b200.runtime import Context, Scene
+from instantradiositytest_b200.workload import Workload
+from oracle import binding as ob
+
+from gpu_harness import RADIANCE_BAR, SELECT_BAR, Lockstep
+
+pytestmark = pytest.mark.gpu
+
+
+def field_meshes(wl):
+    return [i for i, m in enumerate(wl.meshes) if m["geometry_lo"][3] <= 0.5]
+
+
+def random_points(rng, res, n):
+    q = rng.uniform(0.0, res - 1.0, size=(n, 3)).astype(np.float32)
+    q[: n // 8] = np.round(q[: n // 8])  # texel centres, including both edges
+    q[n // 8: n // 4, 0] = np.float32(res - 1)
+    return q
+
+
+def oracle_values(mesh, atlas, q, linear):
+    return np.array([ob.sample_field(mesh, atlas, p, linear) for p in q], np.float32)
+
+
+@pytest.mark.parametrize("preset", [0, 2])
+def test_point_sampler_matches_oracle(cuda, preset):
+    wl = Workload(preset, width=64, height=40)
+    ctx = Context()
+    sc = Scene(ctx, wl.meshes, wl.atlas, wl.sdf_format)
+    rng = np.random.default_rng(5)
+    atlas = wl.atlas_f32()
+    for mi in field_meshes(wl)[:3]:
+        res = int(wl.meshes[mi]["field"][3])
+        q = random_points(rng, res, 2048)
+        got = sc.sample_field(mi, q, L.FIELD_POINT)
+        want = oracle_values(wl.meshes[mi], atlas, q, 0)
+        scale = float(np.abs(want).max())
+        err = float(np.abs(got - want).max())
+        print(f"preset {preset} mesh {mi} (res {res}): point sampler max |diff| {err:.3e} of {scale:.3f}")
+        assert err <= 1e-5 * max(scale, 1.0)
+    sc.close()
+    ctx.close()
+    wl.close()
+
+
+def test_linear_filter_weights_are_the_emulated_fixed_point_weights(cuda):
+    """Ramp atlas: texel (x, y, z) holds x.  Along x the fetched value is
+    x0 + alpha exactly (8-bit alpha, small integers), constant across y and
+    z, so value - floor(value) is the hardware's weight."""
+    wl = Workload(0, width=64, height=40)
+    ramp = np.broadcast_to(np.arange(wl.atlas.shape[2], dtype=np.float32), wl.atlas.shape).copy()
+    ctx = Context()
+    sc = Scene(ctx, wl.meshes, ramp, L.SDF_F32)
+    mi = field_meshes(wl)[0]
+    res = int(wl.meshes[mi]["field"][3])
+    fr = np.linspace(0.0, 1.0, 4097, dtype=np.float32)[:-1]
+    cells = np.array([0, 1, res // 2, res - 3], np.float32)
+    qx = (cells[:, None] + fr[None, :]).reshape(-1).astype(np.float32)
+    q = np.stack([qx, np.full_like(qx, 2.25), np.full_like(qx, 3.75)], -1)
+    got = sc.sample_field(mi, q, L.FIELD_LINEAR)
+    want = oracle_values(wl.meshes[mi], ramp, q, 1)
+    origin = float(wl.meshes[mi]["field"][0])
+    u = ((np.float32(origin) + qx) + np.float32(0.5)) / np.float32(ramp.shape[2])
+    xb = u.astype(np.float64) * ramp.shape[2] - 0.5
+    frac = xb - np.floor(xb)
+    hw = got.astype(np.float64) - np.floor(xb)
+    rules = {"nearest": np.floor(frac * 256 + 0.5) / 256, "truncate": np.floor(frac * 256) / 256}
+    print("hardware weight steps:", np.unique(np.round(hw * 256, 3))[:8], "...",
+          {k: float(np.mean(hw == v)) for k, v in rules.items()})
+    same = got == want
+    print(f"linear weights equal to the emulation at {same.mean():.5f} of {len(q)} points")
+    assert same.mean() >= 0.999
+    sc.close()
+    ctx.close()
+    wl.close()
+
+
+@pytest.mark.parametrize("preset", [0, 2])
+def test_linear_sampler_matches_emulation(cuda, preset):
+    wl = Workload(preset, width=64, height=40)
+    ctx = Context()
+    sc = Scene(ctx, wl.meshes, wl.atlas, wl.sdf_format)
+    rng = np.random.default_rng(9)
+    atlas = wl.atlas_f32()
+    for mi in field_meshes(wl)[:3]:
+        res = int(wl.meshes[mi]["field"][3])
+        q = random_points(rng, res, 2048)
+        got = sc.sample_field(mi, q, L.FIELD_LINEAR)
+        want = oracle_values(wl.meshes[mi], atlas, q, 1)
+        point = oracle_values(wl.meshes[mi], atlas, q, 0)
+        voxel = float(wl.meshes[mi]["grid"][3])
+        err = float(np.abs(got - want).max())
+        print(f"preset {preset} mesh {mi}: linear vs emulation max |diff| {err:.3e}, linear vs point "
+              f"{float(np.abs(got - point).max()):.3e} (voxel diagonal {voxel:.4f})")
+        assert err <= 1e-5 * voxel
+        # the voxel/128 allowance of the bound covers the weight quantisation
+        assert float(np.abs(got - point).max()) <= voxel / 128
+    sc.close()
+    ctx.close()
+    wl.close()
+
+
+@pytest.mark.parametrize("preset,size,formats", [
+    (0, (256, 160), dict()),
+    (2, (240, 150), dict(gbuffer_format=L.GBUFFER_PACKED, radiance_format=L.RADIANCE_F16,
+                         moments_format=L.MOMENTS_F16)),
+])
+def test_linear_field_lockstep_parity(cuda, preset, size, formats):
+    wl = Workload(preset, width=size[0], height=size[1])
+    ls = Lockstep(wl, field_filter=L.FIELD_LINEAR, **formats)
+    rows = [ls.frame(i) for i in range(6)]
+    ls.close()
+    wl.close()
+    worst = {k: (min(r[k] for r in rows) if k.startswith("select") else max(r[k] for r in rows)) for k in rows[0]}
+    print(f"preset {preset} filtered field lockstep", worst)
+    for k, v in worst.items():
+        if k.startswith("select"):
+            assert v >= SELECT_BAR, (k, v)
+        elif k in ("direct", "noisy", "filtered"):
+            assert v <= RADIANCE_BAR, (k, v)

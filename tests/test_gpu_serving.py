@@ -1,6 +1,7 @@
 """The render server (irt_server_*): a session's results are the same alone,
-in a mix of concurrent sessions, and on the plain per-session path; admission
-by HBM bytes; pacing."""
+in a mix of concurrent sessions, and on the plain per-session path, and
+match the oracle; admission by HBM bytes, also of requests that arrive while
+others render; pacing."""
 import time
 
 import numpy as np
@@ -11,6 +12,8 @@ from instantradiositytest_b200 import _lib as L
 from instantradiositytest_b200.runtime import Context, FrameDriver
 from instantradiositytest_b200.serving import Server
 from instantradiositytest_b200.workload import Workload, preset_spec
+
+from gpu_harness import RADIANCE_BAR, SELECT_BAR, Lockstep, outputs, rel_l1
 
 pytestmark = pytest.mark.gpu
 
@@ -89,3 +92,70 @@ def test_frame_pacing(cuda, scenes):
     assert st["frames"] == 12
     assert wall >= 11 / 60.0  # frame k is not started before k / 60 s
     assert st["p99_latency_ms"] < 1000.0
+
+
+def test_served_session_against_the_oracle(cuda, scenes):
+    """A served session's captured frame against the oracle: the same
+    workload runs in lockstep with the oracle on the device-produced
+    G-buffer and VPL pools the server uses (per frame the oracle starts from
+    the session's history), and the served capture equals that session's
+    image bit for bit and the oracle's within the radiance bar."""
+    frames = 6
+    wl = scenes[1]
+    ctx = Context()
+    srv = Server(ctx, 8 << 30, streams=2, frame_rate=0)
+    served = srv.submit(0, 0.0, frames, wl, capture_frame=frames - 1)
+    srv.submit(1, 0.0, frames + 3, scenes[2])  # company on the other stream
+    srv.run()
+    srv.close()
+    ctx.close()
+    ls = Lockstep(wl, gpu_gbuffer=True, gpu_vpls=True)
+    rows = [ls.frame(i) for i in range(frames)]
+    mine = ls.drv.session.buffer(L.BUF_FILTERED, torch.uint8).cpu().numpy()
+    ref = outputs(ls.orc, frames - 1)["filtered"]
+    ls.close()
+    worst = {k: (min(r[k] for r in rows) if k.startswith("select") else max(r[k] for r in rows)) for k in rows[0]}
+    print("served session lockstep", worst)
+    for k, v in worst.items():
+        if k.startswith("select"):
+            assert v >= SELECT_BAR, (k, v)
+        elif k in ("direct", "noisy", "filtered"):
+            assert v <= RADIANCE_BAR, (k, v)
+    assert np.array_equal(served, mine)
+    img = served.view(np.float32).reshape(wl.height, wl.width, 4)[..., :3]
+    assert rel_l1(img, ref) <= RADIANCE_BAR
+
+
+def test_late_arrivals_wait_for_retirements_and_match_alone(cuda, scenes):
+    """Continuous batching: C arrives while A and B are on the GPU and the
+    budget holds two sessions, so C waits; it is admitted when B retires,
+    while A is still rendering, and runs alongside A.  Each session's
+    captured frame equals rendering it alone."""
+    ctx = Context()
+    plan = [(0, 0.0, 40, scenes[0]), (1, 0.0, 6, scenes[1]), (2, 0.03, 10, scenes[2])]  # id, arrival, frames
+    probe = Server(ctx, 1 << 40)
+    need = [probe.request_bytes(wl) for _, _, _, wl in plan]
+    probe.close()
+    # A and B fit together, C does not fit beside both, but fits beside A
+    budget = need[0] + max(need[1], need[2]) + need[2] // 2
+    srv = Server(ctx, budget, streams=2, frame_rate=60.0)
+    times = [np.zeros(3, np.float64) for _ in plan]
+    caps = [srv.submit(i, t, n, wl, capture_frame=n - 1, times=times[i]) for i, t, n, wl in plan]
+    st = srv.run()
+    srv.close()
+    (a_adm, a_done, a_ret), (b_adm, b_done, b_ret), (c_adm, c_done, c_ret) = (tuple(t) for t in times)
+    print("stats", st)
+    print("timeline A", times[0], "B", times[1], "C", times[2])
+    assert st["sessions"] == 3 and st["frames"] == 56 and st["peak_active"] == 2
+    assert c_adm >= b_ret  # C waited for B's bytes
+    assert c_adm > plan[2][1]  # ... after it arrived
+    assert c_adm < a_done  # while A was still rendering
+    assert c_done < a_done  # and its frames ran alongside A's
+    for (i, _, n, wl), cap in zip(plan, caps):
+        solo = Server(ctx, 8 << 30, streams=1, frame_rate=0)
+        alone = solo.submit(i, 0.0, n, wl, capture_frame=n - 1)
+        solo.run()
+        solo.close()
+        assert np.array_equal(alone, cap), i
+        assert np.abs(cap.view(np.float32)).max() > 0
+    ctx.close()

@@ -198,3 +198,35 @@ def test_oracle_small_frames_run_in_both_precisions(precision):
     assert r["count"].max() >= 8
     orc.close()
     wl.close()
+
+
+def test_filtered_field_emulation_weights_and_texel_centres():
+    """The oracle's restatement of the reference's filtered sample_field
+    (src/renderer.rs:277-286): on an atlas whose texels hold their x index,
+    the value is the base texel plus an 8-bit fixed-point weight; at texel
+    centres of a random atlas it equals the point-sampled form; and it never
+    leaves the point-sampled value by more than the voxel/128 allowance the
+    mesh bound carries for fixed-point hardware weights (sdf.wgsl:16-17)."""
+    mesh = np.zeros(1, L.MESH_DTYPE)[0]
+    res = 8
+    mesh["field"] = (4, 0, 0, res)
+    mesh["grid"] = (1.0, 1.0, 1.0, np.sqrt(3.0))
+    dims = (res, res, 16)  # z, y, x
+    ramp = np.broadcast_to(np.arange(dims[2], dtype=np.float32), dims).copy()
+    for fx in np.linspace(0.0, 0.999, 37, dtype=np.float32):
+        v = ob.sample_field(mesh, ramp, (2.0 + fx, 1.5, 3.25), 1)
+        base = 4 + 2
+        assert v - base == pytest.approx(np.floor(float(fx) * 256 + 0.5) / 256, abs=1e-6)
+    rng = np.random.default_rng(3)
+    atlas = rng.uniform(-1, 1, size=dims).astype(np.float32)
+    for _ in range(64):
+        c = rng.integers(0, res, size=3).astype(np.float32)
+        assert ob.sample_field(mesh, atlas, c, 1) == pytest.approx(ob.sample_field(mesh, atlas, c, 0), abs=1e-6)
+    smooth = (np.arange(dims[2], dtype=np.float32)[None, None, :] * 0.3
+              + np.arange(dims[1], dtype=np.float32)[None, :, None] * 0.2
+              + np.arange(dims[0], dtype=np.float32)[:, None, None] * 0.1).astype(np.float32)
+    worst = 0.0
+    for _ in range(256):
+        q = rng.uniform(0, res - 1, size=3).astype(np.float32)
+        worst = max(worst, abs(ob.sample_field(mesh, smooth, q, 1) - ob.sample_field(mesh, smooth, q, 0)))
+    assert worst <= np.sqrt(3.0) / 128
