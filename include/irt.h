@@ -169,6 +169,14 @@ irt_status irt_settings_validate(const irt_settings* s, char* msg, size_t msg_le
 #define IRT_SDF_F32 0
 #define IRT_SDF_F16 1
 
+/* Which build of the library this is: "default", or "checked" for
+ * libirt_checked.so, whose kernels test every index they take from data
+ * (reservoir ids, reprojected and neighbouring pixels, ray-queue and output
+ * slots, leaf-cache object ids) before following it and report a bad one as
+ * IRT_E_DEVICE through irt_session_check instead of faulting.  No
+ * counterpart in the reference (its shaders rely on robust buffer access). */
+const char* irt_build_flavour(void);
+
 /* ---------------------------------------------------------------------------
  * Context, scene, session.
  * ------------------------------------------------------------------------- */

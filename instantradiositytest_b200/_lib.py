@@ -2,7 +2,9 @@
 
 The shared library is built in-tree (``make -C instantradiositytest_b200``) and
 loaded from this directory.  There is no fallback: importing this module
-without the library raises ``ImportError``.
+without the library raises ``ImportError``.  With IRT_LIBRARY=checked in the
+environment the checked build (libirt_checked.so, the same C-ABI with every
+data-dependent index tested in the kernels) is loaded instead.
 """
 from __future__ import annotations
 
@@ -12,7 +14,8 @@ import os
 import numpy as np
 
 _HERE = os.path.dirname(os.path.abspath(__file__))
-LIB_PATH = os.path.join(_HERE, "libirt.so")
+CHECKED_LIB_PATH = os.path.join(_HERE, "libirt_checked.so")
+LIB_PATH = CHECKED_LIB_PATH if os.environ.get("IRT_LIBRARY") == "checked" else os.path.join(_HERE, "libirt.so")
 
 IRT_OK = 0
 IRT_E_INVALID = -1
@@ -181,6 +184,7 @@ _PROTOS = {
     "irt_session_set_profiling": (I32, [P, I32]),
     "irt_session_pass_ms": (I32, [P, C.POINTER(C.c_float)]),
     "irt_session_pass_ms_at": (I32, [P, U32, C.POINTER(C.c_float)]),
+    "irt_build_flavour": (C.c_char_p, []),
     "irt_scene_set_field_filter": (I32, [P, I32]),
     "irt_scene_sample_field": (I32, [P, I32, U32, P, U32, P, P]),
     "irt_svgf_spatial_noalloc": (I32, [C.POINTER(Frame), C.POINTER(GBuffer), I32, I32, U32, P, P, P, P, P,

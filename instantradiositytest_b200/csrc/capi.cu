@@ -369,6 +369,8 @@ irt_status irt_vpl_generate(irt_scene* sc, const irt_workload* wl, const irt_fra
     return IRT_OK;
 }
 
+const char* irt_build_flavour(void) { return IRT_CHECKED ? "checked" : "default"; }
+
 irt_status irt_scene_set_field_filter(irt_scene* sc, int32_t filter) {
     if (!sc) return IRT_E_INVALID;
     if (filter != IRT_FIELD_POINT && filter != IRT_FIELD_LINEAR) {

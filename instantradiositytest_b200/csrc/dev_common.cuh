@@ -342,4 +342,31 @@ __device__ __forceinline__ void raise_error(uint32_t* err, uint32_t code) {
     if (err) atomicOr(err, code);
 }
 
+// The checked build (IRT_CHECKED=1, libirt_checked.so): every index a kernel
+// takes from data rather than from its thread position — reservoir ids into
+// the light table, gathers at reprojected or neighbouring pixels, ray-queue
+// slots and the output slots in the ray records, leaf-cache object ids — is
+// tested against its table before the access.  An index out of range sets
+// IRT_DEVERR_INDEX in the session's error word and the access is skipped, so
+// a bad index is reported instead of faulting (the role compute-sanitizer
+// would play).  In the default build the test compiles away: these indices
+// are in range by construction.
+#ifndef IRT_CHECKED
+#define IRT_CHECKED 0
+#endif
+#define IRT_DEVERR_INDEX 4u  // checked build: an index outside its table
+__device__ __forceinline__ bool index_ok(uint32_t* err, uint64_t i, uint64_t n) {
+#if IRT_CHECKED
+    if (i >= n) {
+        raise_error(err, IRT_DEVERR_INDEX);
+        return false;
+    }
+#else
+    (void)err;
+    (void)i;
+    (void)n;
+#endif
+    return true;
+}
+
 }  // namespace irtd

@@ -110,6 +110,7 @@ struct Px {
             qy >= (int32_t)f.size[1])
             return false;
         size_t q = (size_t)qy * f.size[0] + (size_t)qx;
+        if (!index_ok(a.sc.error, q, (size_t)f.size[0] * f.size[1])) return false;
         float d = __ldg(a.prev_depth + q);
         if (d >= 1.f) return false;
         // world((q + .5) / size, d, previous_inv_vp): the previous frame's
@@ -200,10 +201,12 @@ struct Px {
                 int32_t qx, qy;
                 neighbor(rng, qx, qy);
                 if (qx < 0 || qy < 0 || qx >= (int32_t)f.size[0] || qy >= (int32_t)f.size[1]) continue;
+                if (!index_ok(a.sc.error, (size_t)qy * f.size[0] + (size_t)qx, (size_t)f.size[0] * f.size[1]))
+                    continue;
                 if (!compatible(s, (uint32_t)qx, (uint32_t)qy)) continue;
                 Res previous = res_load(in, (size_t)qy * f.size[0] + (size_t)qx);
                 if (Dom == 0) {
-                    if (previous.target > 0.f) {
+                    if (previous.target > 0.f && index_ok(a.sc.error, previous.id, f.counts[0])) {
                         float target = luminance(direct(s, load_light(a.sc.lights, previous.id)));
                         res_add(r, previous.id, previous.source, target, previous.pdf,
                                 target * normalization(previous) * (float)previous.count, previous.count, previous.age,
@@ -223,7 +226,7 @@ struct Px {
         V3 result = V3{0.f, 0.f, 0.f};
         if (ok) {
             uint32_t dbg = f.flags[2];
-            if (d.target > 0.f && dbg != 2u && dbg < 3u) {
+            if (d.target > 0.f && dbg != 2u && dbg < 3u && index_ok(a.sc.error, d.id, f.counts[0])) {
                 DLight l = load_light(a.sc.lights, d.id);
                 V3 value = direct(s, l);
                 if (luminance(value) > 0.f) {
@@ -363,7 +366,7 @@ __device__ __forceinline__ void spatial_prep_body(const irt_frame& f, const Ligh
         float4 pd = make_float4(0.f, 0.f, 0.f, 0.f);
         uint32_t dbg = f.flags[2];
         if (ok) {
-            if (rd.target > 0.f && dbg != 2u && dbg < 3u) {
+            if (rd.target > 0.f && dbg != 2u && dbg < 3u && index_ok(a.sc.error, rd.id, f.counts[0])) {
                 DLight l = load_light(a.sc.lights, rd.id);
                 V3 value = direct(s, l);
                 if (luminance(value) > 0.f) {

@@ -106,7 +106,7 @@ __device__ __forceinline__ Dist scene_distance_cached(const DevScene& sc, const 
                 done = true;
                 break;
             }
-            if (oid != hint) visit_leaf(sc, f, nodes, objs, p, oid, spacing, r);
+            if (oid != hint && index_ok(sc.error, oid, n)) visit_leaf(sc, f, nodes, objs, p, oid, spacing, r);
         }
         all = !done && sentinel <= wmax(r.best, 0.f);
     }
@@ -162,7 +162,7 @@ __global__ void __launch_bounds__(128, 8) march_kernel(const __grid_constant__ i
                 if (base + cnt >= n_rays) exhausted = true;
                 if (!active) {
                     uint32_t idx = base + (uint32_t)__popc(need & ((1u << lane) - 1u));
-                    if (idx < n_rays) {
+                    if (idx < n_rays && index_ok(sc.error, ray_slot(idx, front, cap), cap)) {
                         ridx = ray_slot(idx, front, cap);
                         const float4* r = reinterpret_cast<const float4*>(rays + ridx);
                         float4 a = __ldg(r), b = __ldg(r + 1);
@@ -202,7 +202,8 @@ __global__ void __launch_bounds__(128, 8) march_kernel(const __grid_constant__ i
             out = march_after(m, d.best, eps, f.sdf[2], max_steps);
         }
         if (out >= 0.f) {
-            vis[__float_as_uint(__ldg(rec).w)] = out;
+            const uint32_t slot = __float_as_uint(__ldg(rec).w);
+            if (index_ok(sc.error, slot, cap)) vis[slot] = out;
             active = false;
         }
     }
@@ -259,7 +260,8 @@ __device__ __forceinline__ bool leaf_may_hold_best(const MNode* nodes, const MOb
 }
 
 // Next object to evaluate for the query, or kNone when the query is complete.
-__device__ __forceinline__ uint32_t query_next(Query& qy, const MNode* nodes, const MObj* objs, uint32_t n) {
+__device__ __forceinline__ uint32_t query_next(Query& qy, const MNode* nodes, const MObj* objs, uint32_t n,
+                                               uint32_t* err) {
     for (;;) {
         const int32_t c = qy.cur;
         if (c < 0) {  // the hint, unconditionally
@@ -273,7 +275,8 @@ __device__ __forceinline__ uint32_t query_next(Query& qy, const MNode* nodes, co
                 return kNone;
             }
             qy.cur = c + 1;
-            if (oid != qy.hint && leaf_may_hold_best(nodes, objs, qy.p, oid, qy.best)) return oid;
+            if (oid != qy.hint && index_ok(err, oid, n) && leaf_may_hold_best(nodes, objs, qy.p, oid, qy.best))
+                return oid;
             continue;
         }
         if (c == kAfterEntries) {  // every cached entry fits: the ones left out may too
@@ -334,7 +337,7 @@ __global__ void __launch_bounds__(128, 8) march_flat_kernel(const __grid_constan
                 if (base + cnt >= n_rays) exhausted = true;
                 if (!active) {
                     uint32_t idx = base + (uint32_t)__popc(need & ((1u << lane) - 1u));
-                    if (idx < n_rays) {
+                    if (idx < n_rays && index_ok(sc.error, ray_slot(idx, front, cap), cap)) {
                         ridx = ray_slot(idx, front, cap);
                         const float4* r = reinterpret_cast<const float4*>(rays + ridx);
                         float4 a = __ldg(r), b = __ldg(r + 1);
@@ -350,7 +353,7 @@ __global__ void __launch_bounds__(128, 8) march_flat_kernel(const __grid_constan
         if (!__any_sync(full, active)) break;
         if (!active) continue;
 
-        uint32_t oid = query_next(qy, nodes, objs, n_obj);
+        uint32_t oid = query_next(qy, nodes, objs, n_obj, sc.error);
         while (oid == kNone) {
             // The query is complete: the march step it feeds (as march_kernel).
             const float4* rec = reinterpret_cast<const float4*>(rays + ridx);
@@ -375,14 +378,15 @@ __global__ void __launch_bounds__(128, 8) march_flat_kernel(const __grid_constan
                 out = march_after(m, qy.best, eps, f.sdf[2], max_steps);
             }
             if (out >= 0.f) {
-                vis[__float_as_uint(__ldg(rec).w)] = out;
+                const uint32_t slot = __float_as_uint(__ldg(rec).w);
+                if (index_ok(sc.error, slot, cap)) vis[slot] = out;
                 active = false;
                 break;
             }
             // the ray's next query
             const V3 q = phase == kEndpoint ? xyz(__ldg(rec + 2)) : march_point(m);
             query_begin(qy, grid, q, phase == kMarch ? m.closest : kNone, n_obj);
-            oid = query_next(qy, nodes, objs, n_obj);
+            oid = query_next(qy, nodes, objs, n_obj, sc.error);
         }
         if (oid != kNone) {
             const float d = object_distance_rec(sc, qy.p, objs[oid]);
@@ -468,7 +472,7 @@ __global__ void __launch_bounds__(128, 8) march_batched_kernel(const MarchGroup*
                     base = __shfl_sync(full, base, leader);
                     if (!active) {
                         uint32_t idx = base + (uint32_t)__popc(need & ((1u << lane) - 1u));
-                        if (idx < n_rays) {
+                        if (idx < n_rays && index_ok(sc.error, ray_slot(idx, front, Q.cap), Q.cap)) {
                             rec = reinterpret_cast<const float4*>(Q.rays + ray_slot(idx, front, Q.cap));
                             float4 a = __ldg(rec), b = __ldg(rec + 1);
                             m.origin = V3{a.x, a.y, a.z};
@@ -519,7 +523,8 @@ __global__ void __launch_bounds__(128, 8) march_batched_kernel(const MarchGroup*
             }
             if (out >= 0.f) {
                 float* vis = queues[lq].vis;
-                vis[__float_as_uint(__ldg(rec).w)] = out;
+                const uint32_t slot = __float_as_uint(__ldg(rec).w);
+                if (index_ok(sc.error, slot, queues[lq].cap)) vis[slot] = out;
                 active = false;
             }
         }

@@ -87,3 +87,15 @@ def test_context_without_device_reports_nodevice():
     h = C.c_void_p()
     cfg = L.Config(0, 0)
     assert L.lib.irt_context_create(C.byref(cfg), C.byref(h)) == L.IRT_E_NODEVICE
+
+
+def test_checked_build_exports_the_same_abi():
+    """libirt_checked.so (kernels test every data-dependent index) is the same
+    C-ABI as libirt.so, and each reports its flavour."""
+    assert os.path.exists(L.CHECKED_LIB_PATH), "build it with make -C instantradiositytest_b200"
+    checked = C.CDLL(L.CHECKED_LIB_PATH)
+    missing = [n for n in declared_functions() if not hasattr(checked, n)]
+    assert not missing, missing
+    checked.irt_build_flavour.restype = C.c_char_p
+    assert checked.irt_build_flavour() == b"checked"
+    assert L.lib.irt_build_flavour() == (b"checked" if L.LIB_PATH == L.CHECKED_LIB_PATH else b"default")
