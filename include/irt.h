@@ -216,8 +216,9 @@ void irt_scene_destroy(irt_scene* scene);
  *   LINEAR: the reference's filtered variant, src/renderer.rs:277-286 (used
  *           there whenever FLOAT32_FILTERABLE is present,
  *           src/renderer.rs:736-739, :914-921, :1470-1471): one hardware
- *           linear fetch at (origin + q + .5) / atlas_dims through a
- *           clamp-to-edge linear sampler.  The filter weights are the
+ *           linear fetch at (origin + q + .5) / atlas_dims (normalised;
+ *           texel coordinate origin + q + .5) through a clamp-to-edge
+ *           linear sampler.  The filter weights are the
  *           hardware's fixed-point ones (8 fractional bits), which the mesh
  *           bound's voxel/128 allowance covers (sdf.wgsl:16-17).
  * irt_scene_set_field_filter takes effect at the scene's next

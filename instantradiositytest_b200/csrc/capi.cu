@@ -114,9 +114,11 @@ irt_status irt_scene_create(irt_context* ctx, const irt_mesh* meshes, uint32_t m
     e = cudaCreateTextureObject(&sc->atlas, &rd, &td, nullptr);
     if (e != cudaSuccess) return fail(cuda_fail(ctx, e, "texture object"));
     // The reference's field_sampler (src/renderer.rs:914-921): linear
-    // min/mag filter, clamp-to-edge, sampled at normalised coordinates.
+    // min/mag filter, clamp-to-edge.  It samples at the normalised
+    // coordinate (origin + q + .5) / dims; this sampler takes the same point
+    // as the texel coordinate origin + q + .5, without the division.
     td.filterMode = cudaFilterModeLinear;
-    td.normalizedCoords = 1;
+    td.normalizedCoords = 0;
     e = cudaCreateTextureObject(&sc->atlas_linear, &rd, &td, nullptr);
     if (e != cudaSuccess) return fail(cuda_fail(ctx, e, "linear texture object"));
     // Corner cells of the field meshes (DevScene::sdf_cells); a mesh's first

@@ -76,11 +76,14 @@ __device__ __forceinline__ float signed_box_distance(V3 p, V3 lo, V3 hi) {
 // z, y, x order as the WGSL loop accumulates them.
 __device__ __forceinline__ float sample_field(const DevScene& sc, const DMesh& m, V3 q) {
     if (sc.filter.linear) {
-        // textureSampleLevel(fields, field_sampler, (vec3<f32>(origin)+q+.5)/vec3<f32>(dims), 0.)
-        // with IEEE rounding in every build, so the coordinate is the reference's.
-        const float u = __fdiv_rn(__fadd_rn(__fadd_rn((float)m.field.x, q.x), .5f), sc.filter.dims[0]);
-        const float v = __fdiv_rn(__fadd_rn(__fadd_rn((float)m.field.y, q.y), .5f), sc.filter.dims[1]);
-        const float w = __fdiv_rn(__fadd_rn(__fadd_rn((float)m.field.z, q.z), .5f), sc.filter.dims[2]);
+        // textureSampleLevel(fields, field_sampler, (vec3<f32>(origin)+q+.5)/vec3<f32>(dims), 0.):
+        // the sampler takes the texel coordinate origin + q + .5 (the
+        // normalised coordinate times the extent), filters between texels
+        // floor(x - .5) and the next with 8-bit fixed-point weights, and
+        // clamps to the atlas edge.
+        const float u = __fadd_rn(__fadd_rn((float)m.field.x, q.x), .5f);
+        const float v = __fadd_rn(__fadd_rn((float)m.field.y, q.y), .5f);
+        const float w = __fadd_rn(__fadd_rn((float)m.field.z, q.z), .5f);
         const float value = tex3D<float>(sc.filter.linear, u, v, w);
         return sc.sdf_f16 ? value * m.lo.w : value;
     }

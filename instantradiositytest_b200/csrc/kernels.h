@@ -8,12 +8,12 @@
 namespace irtd {
 // The reference's filtered variant of sample_field (src/renderer.rs:277-286,
 // chosen there whenever the adapter can filter R32Float textures): one
-// hardware-linear fetch of the atlas at the normalised coordinate
-// (origin + q + .5) / dims, clamp-to-edge, instead of 8 texel loads and f32
-// weights.  linear == 0 selects the point-sampled trilinear of
-// common.wgsl:31-38.
+// hardware-linear fetch of the atlas at the point (origin + q + .5) / dims in
+// normalised coordinates — texel coordinate origin + q + .5 — clamp-to-edge,
+// instead of 8 texel loads and f32 weights.  linear == 0 selects the
+// point-sampled trilinear of common.wgsl:31-38.
 struct FieldFilter {
-    cudaTextureObject_t linear;  // the atlas: normalised coordinates, linear filter, clamp
+    cudaTextureObject_t linear;  // the atlas: texel coordinates, linear filter, clamp
     float dims[3];               // atlas extent in texels
 };
 }  // namespace irtd

@@ -406,21 +406,21 @@ struct Path {
     // The reference's filtered variant of sample_field (src/renderer.rs:
     // 277-286): textureSampleLevel(fields, field_sampler,
     // (vec3(origin) + q + .5) / vec3(dims), 0.) through a clamp-to-edge
-    // linear sampler.  The filter is restated from the linear-filtering
-    // formula of the CUDA C++ Programming Guide ("Texture Fetching"
-    // appendix), which the device sampler implements: at the unnormalised
-    // coordinate x = u * N, x_B = x - 0.5, i = floor(x_B) and
-    // alpha = frac(x_B) held in 9-bit fixed point with 8 fractional bits
-    // (here rounded to the nearest 1/256), and the value is the sum over the
-    // 8 texels of (1 - alpha or alpha) products per axis, clamped to the
-    // atlas edge.  Weighted in the same z, y, x order as sample_field.
+    // linear sampler, i.e. at texel coordinate x = origin + q + .5.  The
+    // filter is restated from the linear-filtering formula of the CUDA C++
+    // Programming Guide ("Texture Fetching" appendix), which the device
+    // sampler implements: x_B = x - 0.5, i = floor(x_B) and alpha = frac(x_B)
+    // held in 9-bit fixed point with 8 fractional bits (here rounded to the
+    // nearest 1/256), and the value is the sum over the 8 texels of
+    // (1 - alpha or alpha) products per axis, clamped to the atlas edge.
+    // Weighted in the same z, y, x order as sample_field.
     T linear_field(const uint32_t origin[3], V3<T> q) const {
         const T qa[3] = {q.x, q.y, q.z};
         int64_t i0[3];
         T alpha[3];
         for (int a = 0; a < 3; a++) {
-            const T u = (((T)origin[a] + qa[a]) + (T).5) / (T)sc.dims[a];
-            const double xb = (double)u * (double)sc.dims[a] - 0.5;
+            const T x = ((T)origin[a] + qa[a]) + (T).5;
+            const double xb = (double)x - 0.5;
             const double fl = std::floor(xb);
             i0[a] = (int64_t)fl;
             alpha[a] = (T)(std::floor((xb - fl) * 256.0 + 0.5) / 256.0);

@@ -81,8 +81,7 @@ def test_linear_filter_weights_are_the_emulated_fixed_point_weights(cuda):
     got = sc.sample_field(mi, q, L.FIELD_LINEAR)
     want = oracle_values(wl.meshes[mi], ramp, q, 1)
     origin = float(wl.meshes[mi]["field"][0])
-    u = ((np.float32(origin) + qx) + np.float32(0.5)) / np.float32(ramp.shape[2])
-    xb = u.astype(np.float64) * ramp.shape[2] - 0.5
+    xb = ((np.float32(origin) + qx) + np.float32(0.5)).astype(np.float64) - 0.5
     frac = xb - np.floor(xb)
     hw = got.astype(np.float64) - np.floor(xb)
     rules = {"nearest": np.floor(frac * 256 + 0.5) / 256, "truncate": np.floor(frac * 256) / 256}
