@@ -223,7 +223,10 @@ void irt_scene_destroy(irt_scene* scene);
  *           bound's voxel/128 allowance covers (sdf.wgsl:16-17).
  * irt_scene_set_field_filter takes effect at the scene's next
  * irt_scene_update (which rebuilds the march's leaf-order cache under the
- * new sampler). */
+ * new sampler).  LINEAR needs an IRT_SDF_F32 atlas, as the reference's
+ * filtered path does (R32Float): the texture unit filters 16-bit texels to a
+ * 16-bit result, whose rounding exceeds the allowance away from surfaces;
+ * IRT_E_INVALID for an F16 atlas. */
 #define IRT_FIELD_POINT 0
 #define IRT_FIELD_LINEAR 1
 irt_status irt_scene_set_field_filter(irt_scene* scene, int32_t filter);
@@ -231,7 +234,8 @@ irt_status irt_scene_set_field_filter(irt_scene* scene, int32_t filter);
  * q (device array of 3*n floats, q in [0, res-1]^3 as mesh_distance forms
  * it, sdf.wgsl:12); out: n floats on the device, dequantised (F16 atlases
  * times the mesh's scale).  The kernels' own sampler, exposed for parity
- * tests of the sampler alone; no counterpart in the reference. */
+ * tests of the sampler alone (LINEAR is evaluated on F16 atlases too, to
+ * measure the 16-bit filter); no counterpart in the reference. */
 irt_status irt_scene_sample_field(const irt_scene* scene, int32_t filter, uint32_t mesh, const float* q,
                                   uint32_t n, float* out, void* stream);
 

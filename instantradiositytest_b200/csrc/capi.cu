@@ -379,6 +379,13 @@ irt_status irt_scene_set_field_filter(irt_scene* sc, int32_t filter) {
         sc->ctx->set_error("unknown field filter");
         return IRT_E_INVALID;
     }
+    if (filter == IRT_FIELD_LINEAR && sc->sdf_f16) {
+        // The texture unit filters 16-bit texels to a 16-bit result: away
+        // from surfaces the rounding exceeds the bound's voxel/128 allowance.
+        // The reference filters R32Float fields only.
+        sc->ctx->set_error("the filtered field sampler needs an f32 SDF atlas (16-bit texels filter to 16-bit values)");
+        return IRT_E_INVALID;
+    }
     sc->field_linear_requested = filter == IRT_FIELD_LINEAR;
     return IRT_OK;
 }

@@ -1,10 +1,10 @@
 // march.cu — persistent soft-shadow march over the ray queue.
 //
-// visibility() of sdf.wgsl:61-81 restated as a per-lane state machine whose
-// every iteration issues exactly one scene_distance query: the clearance
-// query at the surface point, the endpoint clearance query for VPL rays, then
-// up to sdf_max_steps march steps.  A lane that finishes its ray refills from
-// the queue on the next iteration (warp-aggregated atomic fetch).
+// visibility() of sdf.wgsl:61-81 restated as a per-lane state machine over
+// its scene_distance queries: the clearance query at the surface point, the
+// endpoint clearance query for VPL rays, then up to sdf_max_steps march
+// steps.  A lane that finishes its ray refills from the queue (warp-
+// aggregated atomic fetch).
 //
 // scene_distance (sdf.wgsl:42-60) returns the minimum object distance: the
 // walk skips a subtree only when its box bound exceeds the current best, and
@@ -20,12 +20,13 @@
 // Per object the arithmetic is object_distance()'s, evaluated on records
 // staged in shared memory.
 //
+// The loop is flattened to one object per lane and iteration (see Query):
+// lanes at different stages of their queries evaluate objects together.
+//
 // This file is built twice: as is (IEEE division and square root, the
 // arithmetic of the per-pixel visibility()), and through march_fast.cu with
 // approximate division and square root for the default fast march.
 #include <cuda_runtime.h>
-
-#include <cstdlib>
 
 #include "dev_sdf.cuh"
 #include "kernels.h"
@@ -61,166 +62,20 @@ struct Grid {
     float ox, oy, oz, ix, iy, iz;
 };
 
-// Leaf `oid` (box of BVH node `leaf`) against the best so far: the walk's
-// pruning test, then the object's distance.
-__device__ __forceinline__ void visit_leaf(const DevScene& sc, const irt_frame& f, const MNode* nodes,
-                                           const MObj* objs, V3 p, uint32_t oid, bool spacing, Dist& r) {
-    const MObj& o = objs[oid];
-    const uint32_t leaf = __float_as_uint(o.meta.w);
-    const float4 a = nodes[leaf].a, b = nodes[leaf].b;
-    V3 delta = vmax(vmax(V3{a.x, a.y, a.z} - p, p - V3{b.x, b.y, b.z}), V3{0.f, 0.f, 0.f});
-    V3 lb = delta * .9998f;
-    float bb = wmax(r.best, 0.f);
-    if (dot(lb, lb) > bb * bb) return;
-    float d = object_distance_rec(sc, p, o);
-    if (d < r.best) {
-        r.best = d;
-        r.voxel = spacing ? o.meta.y : f.sdf[1];
-        r.closest = oid;
-    }
-}
-
-__device__ __forceinline__ Dist scene_distance_cached(const DevScene& sc, const irt_frame& f, const Grid& g,
-                                                      const MNode* nodes, const MObj* objs, V3 p, uint32_t hint,
-                                                      bool spacing) {
-    const uint32_t n = f.counts[3];
-    Dist r{1e20f, f.sdf[1], hint};
-    if (hint < n) {
-        const MObj& o = objs[hint];
-        r.best = object_distance_rec(sc, p, o);
-        if (spacing) r.voxel = o.meta.y;
-    }
-    const float fx = (p.x - g.ox) * g.ix, fy = (p.y - g.oy) * g.iy, fz = (p.z - g.oz) * g.iz;
-    const float G = (float)kGridRes;
-    bool all = !(fx >= 0.f && fy >= 0.f && fz >= 0.f && fx < G && fy < G && fz < G);
-    if (!all) {
-        const uint32_t cell = ((uint32_t)fz * kGridRes + (uint32_t)fy) * kGridRes + (uint32_t)fx;
-        const uint4* c = g.cells + (size_t)cell * (kCellWords / 4);
-        const uint32_t* cw = reinterpret_cast<const uint32_t*>(c);
-        const float sentinel = __uint_as_float(__ldg(cw + 12));
-        bool done = false;
-#pragma unroll 1
-        for (int j = 0; j < (int)kCellEntries; j++) {
-            const uint32_t oid = (__ldg(cw + (j >> 1)) >> ((j & 1) * 16)) & 0xffffu;
-            if (__uint_as_float(__ldg(cw + 4 + j)) > wmax(r.best, 0.f) || oid == 0xffffu) {
-                done = true;
-                break;
-            }
-            if (oid != hint && index_ok(sc.error, oid, n)) visit_leaf(sc, f, nodes, objs, p, oid, spacing, r);
-        }
-        all = !done && sentinel <= wmax(r.best, 0.f);
-    }
-    if (all) {
-        for (uint32_t oid = 0; oid < n; oid++)
-            if (oid != hint) visit_leaf(sc, f, nodes, objs, p, oid, spacing, r);
-    }
-    return r;
-}
-
-__global__ void __launch_bounds__(128, 8) march_kernel(const __grid_constant__ irt_frame f, const DevScene sc,
-                                                    const float4* __restrict__ march_scene, uint32_t scene_vec4,
-                                                    const Grid grid, const RayRecord* __restrict__ rays,
-                                                    uint32_t* counters, float* __restrict__ vis) {
-    extern __shared__ float4 smem[];
-    for (uint32_t i = threadIdx.x; i < scene_vec4; i += blockDim.x) smem[i] = __ldg(march_scene + i);
-    __syncthreads();
-    const uint32_t n_obj = f.counts[3];
-    const MNode* nodes = reinterpret_cast<const MNode*>(smem);
-    const MObj* objs = reinterpret_cast<const MObj*>(smem + 2 * (2 * n_obj - 1));
-
-    const uint32_t front = *(volatile uint32_t*)&counters[0];
-    const uint32_t n_rays = front + *(volatile uint32_t*)&counters[2];
-    const uint32_t cap = 2u * f.size[0] * f.size[1];
-    const unsigned full = 0xffffffffu;
-    const int lane = threadIdx.x & 31;
-    const float eps = f.sdf[1];
-    const uint32_t max_steps = to_u32(f.sdf[0]);
-
-    bool active = false;
-    bool exhausted = false;  // warp-uniform: the queue has no rays left
-    // A lane keeps its ray's index and re-reads the record's target, endpoint
-    // normal and output slot where a phase needs them (L1/L2 hits), which
-    // keeps fewer values live across the distance query.
-    uint32_t phase = kClear, ridx = 0;
-    MarchState m;
-    m.closest = kNone;
-    m.origin = V3{0.f, 0.f, 0.f};  // surface point until the clearance query
-    m.dir = V3{0.f, 0.f, 0.f};     // surface normal until the march begins
-    m.t = m.limit = 0.f;
-    m.result = 1.f;
-    m.previous = 1e20f;
-    m.step = 0;
-    for (;;) {
-        if (!exhausted) {
-            unsigned need = __ballot_sync(full, !active);
-            if (need) {
-                int leader = __ffs(need) - 1;
-                uint32_t cnt = (uint32_t)__popc(need);
-                uint32_t base = 0;
-                if (lane == leader) base = atomicAdd(&counters[1], cnt);
-                base = __shfl_sync(full, base, leader);
-                if (base + cnt >= n_rays) exhausted = true;
-                if (!active) {
-                    uint32_t idx = base + (uint32_t)__popc(need & ((1u << lane) - 1u));
-                    if (idx < n_rays && index_ok(sc.error, ray_slot(idx, front, cap), cap)) {
-                        ridx = ray_slot(idx, front, cap);
-                        const float4* r = reinterpret_cast<const float4*>(rays + ridx);
-                        float4 a = __ldg(r), b = __ldg(r + 1);
-                        m.origin = V3{a.x, a.y, a.z};
-                        m.dir = V3{b.x, b.y, b.z};
-                        phase = kClear;
-                        active = true;
-                    }
-                }
-            }
-        }
-        if (!__any_sync(full, active)) break;
-        if (!active) continue;
-
-        const float4* rec = reinterpret_cast<const float4*>(rays + ridx);
-        V3 q = phase == kClear ? m.origin : (phase == kEndpoint ? xyz(__ldg(rec + 2)) : march_point(m));
-        uint32_t hint = phase == kMarch ? m.closest : kNone;
-        Dist d = scene_distance_cached(sc, f, grid, nodes, objs, q, hint, phase != kMarch);
-
-        float out = -1.f;
-        if (phase == kClear) {
-            m.closest = d.closest;
-            m.origin = m.origin + m.dir * clearance_epsilon(eps, d.voxel);
-            const V3 endn = xyz(__ldg(rec + 3));
-            if (dot(endn, endn) > .5f) {
-                phase = kEndpoint;
-            } else {
-                phase = kMarch;
-                out = march_begin(m, xyz(__ldg(rec + 2)), eps, max_steps);
-            }
-        } else if (phase == kEndpoint) {
-            phase = kMarch;
-            const V3 target = xyz(__ldg(rec + 2)), endn = xyz(__ldg(rec + 3));
-            out = march_begin(m, target + endn * clearance_epsilon(eps, d.voxel), eps, max_steps);
-        } else {
-            m.closest = d.closest;
-            out = march_after(m, d.best, eps, f.sdf[2], max_steps);
-        }
-        if (out >= 0.f) {
-            const uint32_t slot = __float_as_uint(__ldg(rec).w);
-            if (index_ok(sc.error, slot, cap)) vis[slot] = out;
-            active = false;
-        }
-    }
-}
-
 // The march as one flattened loop: every iteration each lane evaluates at
 // most one object, the next candidate of its current distance query — the
 // hint object first (the previous closest, as scene_distance seeds it), then
 // the leaf-order cache entries of the query point's cell that survive the
-// walk's pruning tests, then (rarely) every leaf.  A lane whose query has no
-// candidate left completes it (the march step of sdf.wgsl:61-81), starts its
-// ray's next query, or takes a new ray, and finds that query's first
-// candidate within the same iteration.  Candidate order and pruning per
-// query are exactly scene_distance_cached's, so results are unchanged; the
-// object evaluations of lanes at different stages of their queries (a hint,
-// a second leaf, the first leaf of a new ray) issue together instead of in
-// separate divergent sections.
+// walk's pruning tests (stopping at the first entry whose bound exceeds the
+// best), then every leaf when the cached entries may not hold the minimum
+// or the point is outside the grid.  A lane whose query has no candidate
+// left completes it (the step of sdf.wgsl:61-81 it feeds), starts its ray's
+// next query or takes a new ray, and finds that query's first candidate in
+// the same iteration.  So the object evaluations of lanes at different
+// stages of their queries (a hint, a second leaf, the first leaf of a new
+// ray) issue together instead of in separate divergent sections; per query
+// the candidates and their order are the same as a walk of one query at a
+// time, so the results are too.
 struct Query {
     V3 p;
     float best;
@@ -293,10 +148,65 @@ __device__ __forceinline__ uint32_t query_next(Query& qy, const MNode* nodes, co
     }
 }
 
-__global__ void __launch_bounds__(128, 8) march_flat_kernel(const __grid_constant__ irt_frame f, const DevScene sc,
-                                                         const float4* __restrict__ march_scene, uint32_t scene_vec4,
-                                                         const Grid grid, const RayRecord* __restrict__ rays,
-                                                         uint32_t* counters, float* __restrict__ vis) {
+// Object `oid`'s distance folded into the query (the hint sets the best
+// unconditionally, as scene_distance seeds it).
+__device__ __forceinline__ void query_eval(Query& qy, const DevScene& sc, const MObj* objs, uint32_t oid) {
+    const float d = object_distance_rec(sc, qy.p, objs[oid]);
+    if (oid == qy.hint || d < qy.best) {
+        qy.best = d;
+        qy.closest = oid;
+    }
+}
+
+// A completed query's step of visibility() (sdf.wgsl:61-81): after the
+// clearance query the ray leaves the surface (and, for a VPL, queries the
+// endpoint's clearance), after the endpoint query the march begins, after a
+// march query the penumbra update.  Returns the visibility once the ray is
+// resolved, else -1 with the ray's next query begun.
+__device__ __forceinline__ float query_finish(Query& qy, MarchState& m, uint32_t& phase, const float4* rec,
+                                              const Grid& grid, const MObj* objs, uint32_t n_obj, float eps, float k,
+                                              uint32_t max_steps) {
+    const float voxel = (phase != kMarch && qy.closest < n_obj) ? objs[qy.closest].meta.y : eps;
+    float out = -1.f;
+    if (phase == kClear) {
+        m.closest = qy.closest;
+        m.origin = m.origin + m.dir * clearance_epsilon(eps, voxel);
+        const V3 endn = xyz(__ldg(rec + 3));
+        if (dot(endn, endn) > .5f) {
+            phase = kEndpoint;
+        } else {
+            phase = kMarch;
+            out = march_begin(m, xyz(__ldg(rec + 2)), eps, max_steps);
+        }
+    } else if (phase == kEndpoint) {
+        phase = kMarch;
+        const V3 target = xyz(__ldg(rec + 2)), endn = xyz(__ldg(rec + 3));
+        out = march_begin(m, target + endn * clearance_epsilon(eps, voxel), eps, max_steps);
+    } else {
+        m.closest = qy.closest;
+        out = march_after(m, qy.best, eps, k, max_steps);
+    }
+    if (out < 0.f) {
+        const V3 q = phase == kEndpoint ? xyz(__ldg(rec + 2)) : march_point(m);
+        query_begin(qy, grid, q, phase == kMarch ? m.closest : kNone, n_obj);
+    }
+    return out;
+}
+
+__device__ __forceinline__ void march_reset(MarchState& m) {
+    m.closest = kNone;
+    m.origin = V3{0.f, 0.f, 0.f};
+    m.dir = V3{0.f, 0.f, 0.f};
+    m.t = m.limit = 0.f;
+    m.result = 1.f;
+    m.previous = 1e20f;
+    m.step = 0;
+}
+
+__global__ void __launch_bounds__(128, 8) march_kernel(const __grid_constant__ irt_frame f, const DevScene sc,
+                                                    const float4* __restrict__ march_scene, uint32_t scene_vec4,
+                                                    const Grid grid, const RayRecord* __restrict__ rays,
+                                                    uint32_t* counters, float* __restrict__ vis) {
     extern __shared__ float4 smem[];
     for (uint32_t i = threadIdx.x; i < scene_vec4; i += blockDim.x) smem[i] = __ldg(march_scene + i);
     __syncthreads();
@@ -314,15 +224,12 @@ __global__ void __launch_bounds__(128, 8) march_flat_kernel(const __grid_constan
 
     bool active = false;
     bool exhausted = false;  // warp-uniform: the queue has no rays left
+    // A lane keeps its ray's index and re-reads the record's target, endpoint
+    // normal and output slot where a step needs them (L1/L2 hits), which
+    // keeps fewer values live across the loop.
     uint32_t phase = kClear, ridx = 0;
     MarchState m;
-    m.closest = kNone;
-    m.origin = V3{0.f, 0.f, 0.f};
-    m.dir = V3{0.f, 0.f, 0.f};
-    m.t = m.limit = 0.f;
-    m.result = 1.f;
-    m.previous = 1e20f;
-    m.step = 0;
+    march_reset(m);
     Query qy;
     qy.cur = kQueryDone;
     for (;;) {
@@ -341,11 +248,11 @@ __global__ void __launch_bounds__(128, 8) march_flat_kernel(const __grid_constan
                         ridx = ray_slot(idx, front, cap);
                         const float4* r = reinterpret_cast<const float4*>(rays + ridx);
                         float4 a = __ldg(r), b = __ldg(r + 1);
-                        m.origin = V3{a.x, a.y, a.z};
-                        m.dir = V3{b.x, b.y, b.z};
+                        m.origin = V3{a.x, a.y, a.z};  // surface point until the clearance query
+                        m.dir = V3{b.x, b.y, b.z};     // surface normal until the march begins
                         phase = kClear;
                         active = true;
-                        query_begin(qy, grid, m.origin, kNone, n_obj);  // the clearance query
+                        query_begin(qy, grid, m.origin, kNone, n_obj);
                     }
                 }
             }
@@ -355,55 +262,24 @@ __global__ void __launch_bounds__(128, 8) march_flat_kernel(const __grid_constan
 
         uint32_t oid = query_next(qy, nodes, objs, n_obj, sc.error);
         while (oid == kNone) {
-            // The query is complete: the march step it feeds (as march_kernel).
             const float4* rec = reinterpret_cast<const float4*>(rays + ridx);
-            const float voxel = (phase != kMarch && qy.closest < n_obj) ? objs[qy.closest].meta.y : eps;
-            float out = -1.f;
-            if (phase == kClear) {
-                m.closest = qy.closest;
-                m.origin = m.origin + m.dir * clearance_epsilon(eps, voxel);
-                const V3 endn = xyz(__ldg(rec + 3));
-                if (dot(endn, endn) > .5f) {
-                    phase = kEndpoint;
-                } else {
-                    phase = kMarch;
-                    out = march_begin(m, xyz(__ldg(rec + 2)), eps, max_steps);
-                }
-            } else if (phase == kEndpoint) {
-                phase = kMarch;
-                const V3 target = xyz(__ldg(rec + 2)), endn = xyz(__ldg(rec + 3));
-                out = march_begin(m, target + endn * clearance_epsilon(eps, voxel), eps, max_steps);
-            } else {
-                m.closest = qy.closest;
-                out = march_after(m, qy.best, eps, f.sdf[2], max_steps);
-            }
+            const float out = query_finish(qy, m, phase, rec, grid, objs, n_obj, eps, f.sdf[2], max_steps);
             if (out >= 0.f) {
                 const uint32_t slot = __float_as_uint(__ldg(rec).w);
                 if (index_ok(sc.error, slot, cap)) vis[slot] = out;
                 active = false;
                 break;
             }
-            // the ray's next query
-            const V3 q = phase == kEndpoint ? xyz(__ldg(rec + 2)) : march_point(m);
-            query_begin(qy, grid, q, phase == kMarch ? m.closest : kNone, n_obj);
             oid = query_next(qy, nodes, objs, n_obj, sc.error);
         }
-        if (oid != kNone) {
-            const float d = object_distance_rec(sc, qy.p, objs[oid]);
-            if (oid == qy.hint || d < qy.best) {  // the hint sets the best unconditionally
-                qy.best = d;
-                qy.closest = oid;
-            }
-        }
+        if (oid != kNone) query_eval(qy, sc, objs, oid);
     }
 }
 
 // Batched march: for each scene group the CTA stages the group record and
 // its compact scene in shared memory, then its warps consume the group's ray
-// queues (one per view) in order with the same per-lane state machine; a
-// lane keeps the address of its ray record and the index of the queue it
-// came from, and re-reads the record's target, endpoint normal and output
-// slot where a phase needs them (as march_kernel does).
+// queues (one per view) in order with the same flattened loop; a lane keeps
+// the address of its ray record and the index of the queue it came from.
 constexpr uint32_t kGroupVec4 = (uint32_t)((sizeof(MarchGroup) + 15) / 16);
 
 __global__ void __launch_bounds__(128, 8) march_batched_kernel(const MarchGroup* __restrict__ groups, uint32_t n_groups,
@@ -453,13 +329,9 @@ __global__ void __launch_bounds__(128, 8) march_batched_kernel(const MarchGroup*
         uint32_t phase = kClear, lq = 0;
         const float4* rec = nullptr;
         MarchState m;
-        m.closest = kNone;
-        m.origin = V3{0.f, 0.f, 0.f};
-        m.dir = V3{0.f, 0.f, 0.f};
-        m.t = m.limit = 0.f;
-        m.result = 1.f;
-        m.previous = 1e20f;
-        m.step = 0;
+        march_reset(m);
+        Query qy;
+        qy.cur = kQueryDone;
         for (;;) {
             if (!exhausted) {
                 unsigned need = __ballot_sync(full, !active);
@@ -480,6 +352,7 @@ __global__ void __launch_bounds__(128, 8) march_batched_kernel(const MarchGroup*
                             phase = kClear;
                             lq = q;
                             active = true;
+                            query_begin(qy, grid, m.origin, kNone, n_obj);
                         }
                     }
                     if (base + cnt >= n_rays) {  // this queue is used up: the next view's
@@ -498,35 +371,19 @@ __global__ void __launch_bounds__(128, 8) march_batched_kernel(const MarchGroup*
             }
             if (!active) continue;
 
-            V3 qp = phase == kClear ? m.origin : (phase == kEndpoint ? xyz(__ldg(rec + 2)) : march_point(m));
-            uint32_t hint = phase == kMarch ? m.closest : kNone;
-            Dist d = scene_distance_cached(sc, f, grid, nodes, objs, qp, hint, phase != kMarch);
-
-            float out = -1.f;
-            if (phase == kClear) {
-                m.closest = d.closest;
-                m.origin = m.origin + m.dir * clearance_epsilon(eps, d.voxel);
-                const V3 endn = xyz(__ldg(rec + 3));
-                if (dot(endn, endn) > .5f) {
-                    phase = kEndpoint;
-                } else {
-                    phase = kMarch;
-                    out = march_begin(m, xyz(__ldg(rec + 2)), eps, max_steps);
+            uint32_t oid = query_next(qy, nodes, objs, n_obj, sc.error);
+            while (oid == kNone) {
+                const float out = query_finish(qy, m, phase, rec, grid, objs, n_obj, eps, f.sdf[2], max_steps);
+                if (out >= 0.f) {
+                    float* vis = queues[lq].vis;
+                    const uint32_t slot = __float_as_uint(__ldg(rec).w);
+                    if (index_ok(sc.error, slot, queues[lq].cap)) vis[slot] = out;
+                    active = false;
+                    break;
                 }
-            } else if (phase == kEndpoint) {
-                phase = kMarch;
-                const V3 target = xyz(__ldg(rec + 2)), endn = xyz(__ldg(rec + 3));
-                out = march_begin(m, target + endn * clearance_epsilon(eps, d.voxel), eps, max_steps);
-            } else {
-                m.closest = d.closest;
-                out = march_after(m, d.best, eps, f.sdf[2], max_steps);
+                oid = query_next(qy, nodes, objs, n_obj, sc.error);
             }
-            if (out >= 0.f) {
-                float* vis = queues[lq].vis;
-                const uint32_t slot = __float_as_uint(__ldg(rec).w);
-                if (index_ok(sc.error, slot, queues[lq].cap)) vis[slot] = out;
-                active = false;
-            }
+            if (oid != kNone) query_eval(qy, sc, objs, oid);
         }
     }
 }
@@ -578,25 +435,6 @@ cudaError_t IRT_MARCH_LAUNCH(const MarchLaunch& M, cudaStream_t st) {
     g.ix = M.grid_inv[0];
     g.iy = M.grid_inv[1];
     g.iz = M.grid_inv[2];
-    static const bool flat = getenv("IRT_MARCH_FLAT") && getenv("IRT_MARCH_FLAT")[0] == '1';
-    if (flat) {
-        thread_local int flat_device = -1;
-        thread_local uint32_t flat_smem = 0;
-        thread_local int flat_blocks = 0;
-        if (smem != flat_smem || device != flat_device) {
-            flat_device = device;
-            cudaError_t e = cudaFuncSetAttribute(march_flat_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                                 (int)smem);
-            if (e != cudaSuccess) return e;
-            e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&flat_blocks, march_flat_kernel, 128, smem);
-            if (e != cudaSuccess) return e;
-            if (flat_blocks < 1) return cudaErrorInvalidConfiguration;
-            flat_smem = smem;
-        }
-        march_flat_kernel<<<M.num_sms * flat_blocks, 128, smem, st>>>(*M.frame, sc, M.march_scene, smem / 16, g,
-                                                                       M.rays, M.ray_counters, M.vis);
-        return cudaGetLastError();
-    }
     march_kernel<<<M.num_sms * blocks_per_sm, 128, smem, st>>>(*M.frame, sc, M.march_scene, smem / 16, g, M.rays,
                                                                 M.ray_counters, M.vis);
     return cudaGetLastError();

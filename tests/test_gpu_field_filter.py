@@ -95,8 +95,9 @@ def test_linear_filter_weights_are_the_emulated_fixed_point_weights(cuda):
     wl.close()
 
 
-@pytest.mark.parametrize("preset", [0, 2])
+@pytest.mark.parametrize("preset", [0, 1])
 def test_linear_sampler_matches_emulation(cuda, preset):
+    """Random points of the f32 fields of the 12- and 24-mesh rooms."""
     wl = Workload(preset, width=64, height=40)
     ctx = Context()
     sc = Scene(ctx, wl.meshes, wl.atlas, wl.sdf_format)
@@ -120,14 +121,34 @@ def test_linear_sampler_matches_emulation(cuda, preset):
     wl.close()
 
 
-@pytest.mark.parametrize("preset,size,formats", [
-    (0, (256, 160), dict()),
-    (2, (240, 150), dict(gbuffer_format=L.GBUFFER_PACKED, radiance_format=L.RADIANCE_F16,
-                         moments_format=L.MOMENTS_F16)),
-])
-def test_linear_field_lockstep_parity(cuda, preset, size, formats):
+def test_linear_sampler_is_refused_for_f16_atlases(cuda):
+    """The texture unit filters 16-bit texels to a 16-bit result; on the
+    mixed-precision room that rounding exceeds the bound's voxel/128
+    allowance away from surfaces, so a scene with an f16 atlas refuses the
+    filtered sampler (the reference filters R32Float fields only)."""
+    wl = Workload(2, width=64, height=40)
+    ctx = Context()
+    sc = Scene(ctx, wl.meshes, wl.atlas, wl.sdf_format)
+    mi = field_meshes(wl)[0]
+    res = int(wl.meshes[mi]["field"][3])
+    q = random_points(np.random.default_rng(2), res, 2048)
+    got = sc.sample_field(mi, q, L.FIELD_LINEAR)
+    point = sc.sample_field(mi, q, L.FIELD_POINT)
+    voxel = float(wl.meshes[mi]["grid"][3])
+    print(f"f16 atlas: filtered vs point max |diff| {float(np.abs(got - point).max()):.3e}, voxel/128 "
+          f"{voxel / 128:.3e}")
+    with pytest.raises(L.IrtError):
+        sc.set_field_filter(L.FIELD_LINEAR)
+    sc.set_field_filter(L.FIELD_POINT)
+    sc.close()
+    ctx.close()
+    wl.close()
+
+
+@pytest.mark.parametrize("preset,size", [(0, (256, 160)), (1, (240, 150))])
+def test_linear_field_lockstep_parity(cuda, preset, size):
     wl = Workload(preset, width=size[0], height=size[1])
-    ls = Lockstep(wl, field_filter=L.FIELD_LINEAR, **formats)
+    ls = Lockstep(wl, field_filter=L.FIELD_LINEAR)
     rows = [ls.frame(i) for i in range(6)]
     ls.close()
     wl.close()
