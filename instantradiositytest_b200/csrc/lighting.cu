@@ -13,8 +13,6 @@
 // row, so every own-pixel access is a coalesced 128-bit vector access).
 #include <cuda_runtime.h>
 
-#include <cstdlib>
-
 #include <type_traits>
 
 #include "dev_sdf.cuh"
@@ -44,22 +42,12 @@ struct LightArgs {
     const float4* feat;       // decoded (normal, rough), (colour, metal) per pixel, or null
 };
 
-// A block's neighbourhood staged in shared memory for the spatial pass:
-// per pixel of the block grown by the spatial radius, its world position
-// (w = 1 where depth < 1) and its normalised normal — the two values
-// compatible() reads of a neighbour, formed by the same operations.
-struct NbrTile {
-    const float4* t;  // 2 float4 per pixel, row-major, `w` pixels a row
-    int32_t x0, y0, w;
-};
-
 template <class G>
 struct Px {
     const irt_frame& f;
     const LightArgs<G>& a;
     uint32_t x, y;
     size_t id;
-    const NbrTile* tile = nullptr;
     __device__ __forceinline__ Px(const irt_frame& fr, const LightArgs<G>& ar, uint32_t px, uint32_t py)
         : f(fr), a(ar), x(px), y(py), id((size_t)py * fr.size[0] + px) {}
 
@@ -102,14 +90,6 @@ struct Px {
     }
     // lighting.wgsl:36-40
     __device__ __forceinline__ bool compatible(const Surface& s, uint32_t qx, uint32_t qy) const {
-        if (tile) {
-            const int32_t k = ((int32_t)qy - tile->y0) * tile->w + ((int32_t)qx - tile->x0);
-            const float4 P = tile->t[2 * k];
-            if (P.w == 0.f) return false;
-            const V3 n = xyz(tile->t[2 * k + 1]);
-            return dot(s.n, n) > f.temporal[2] &&
-                   distance(s.p, xyz(P)) < f.temporal[1] * wmax(distance(s.p, camera()), 1.f);
-        }
         size_t q = (size_t)qy * f.size[0] + qx;
         float d = a.g.d(q);
         if (d >= 1.f) return false;
@@ -367,15 +347,13 @@ __global__ void __launch_bounds__(256) shade_kernel(const __grid_constant__ irt_
 constexpr uint32_t kVplCounter = 0, kLightCounter = 2;
 
 template <class G, class R>
-__device__ __forceinline__ void spatial_prep_body(const irt_frame& f, const LightArgs<G>& a, uint32_t x, uint32_t y,
-                                                  const NbrTile* tile = nullptr) {
+__device__ __forceinline__ void spatial_prep_body(const irt_frame& f, const LightArgs<G>& a, uint32_t x, uint32_t y) {
     const bool in = x < f.size[0] && y < f.size[1];
     bool ray_d = false, ray_i = false;
     V3 sp{0.f, 0.f, 0.f}, sn{0.f, 0.f, 0.f}, lpos{0.f, 0.f, 0.f}, vpos{0.f, 0.f, 0.f}, vnrm{0.f, 0.f, 0.f};
     size_t id = 0;
     if (in) {
         Px<G> px(f, a, x, y);
-        px.tile = tile;
         id = px.id;
         bool ok = px.valid();
         Surface s;
@@ -464,40 +442,6 @@ template <class G, class R>
 __global__ void __launch_bounds__(256, 4) spatial_prep_kernel(const __grid_constant__ irt_frame f,
                                                            const __grid_constant__ LightArgs<G> a) {
     spatial_prep_body<G, R>(f, a, blockIdx.x * blockDim.x + threadIdx.x, blockIdx.y * blockDim.y + threadIdx.y);
-}
-
-// spatial_prep with the block's neighbourhood (the 32x8 block grown by the
-// spatial radius, at most kNbrR pixels) staged in shared memory first: the
-// neighbour tests read positions and normals from there instead of gathering
-// depth, guide and normal from global memory per tap.
-constexpr int32_t kNbrR = 12;
-constexpr int32_t kNbrW = 32 + 2 * kNbrR, kNbrH = 8 + 2 * kNbrR;
-constexpr uint32_t kNbrTileBytes = 2u * 16u * kNbrW * kNbrH;
-
-template <class G, class R>
-__global__ void __launch_bounds__(256, 3) spatial_prep_tiled_kernel(const __grid_constant__ irt_frame f,
-                                                                 const __grid_constant__ LightArgs<G> a) {
-    extern __shared__ float4 nbr[];
-    const int32_t x0 = (int32_t)(blockIdx.x * 32) - kNbrR, y0 = (int32_t)(blockIdx.y * 8) - kNbrR;
-    const int32_t W = (int32_t)f.size[0], H = (int32_t)f.size[1];
-    Px<G> stage(f, a, 0, 0);
-    for (int32_t i = threadIdx.y * 32 + threadIdx.x; i < kNbrW * kNbrH; i += 256) {
-        const int32_t qx = x0 + i % kNbrW, qy = y0 + i / kNbrW;
-        float4 P = make_float4(0.f, 0.f, 0.f, 0.f), N = P;
-        if (qx >= 0 && qy >= 0 && qx < W && qy < H) {
-            const size_t q = (size_t)qy * (size_t)W + (size_t)qx;
-            if (a.g.d(q) < 1.f) {
-                const V3 p = stage.position(q), n = normalize(stage.normal_of(q));
-                P = make_float4(p.x, p.y, p.z, 1.f);
-                N = make_float4(n.x, n.y, n.z, 0.f);
-            }
-        }
-        nbr[2 * i] = P;
-        nbr[2 * i + 1] = N;
-    }
-    __syncthreads();
-    const NbrTile tile{nbr, x0, y0, kNbrW};
-    spatial_prep_body<G, R>(f, a, blockIdx.x * blockDim.x + threadIdx.x, blockIdx.y * blockDim.y + threadIdx.y, &tile);
 }
 
 // resolve_direct / resolve_indirect outputs from contribution x visibility:
@@ -701,21 +645,7 @@ static cudaError_t launch_typed(const LightingLaunch& L, int stage, cudaStream_t
     switch (stage) {
     case kStageReuse: reuse_kernel<G><<<grid, block, 0, st>>>(f, a, L.keep_candidates); break;
     case kStageShade: shade_kernel<G, R><<<grid, block, 0, st>>>(f, a); break;
-    case kStageSpatial: {
-        static const bool tiled = getenv("IRT_SPATIAL_TILE") && getenv("IRT_SPATIAL_TILE")[0] == '1';
-        if (tiled && f.restir[3] <= (uint32_t)kNbrR) {
-            thread_local bool configured = false;
-            if (!configured) {
-                cudaError_t e = cudaFuncSetAttribute(spatial_prep_tiled_kernel<G, R>,
-                                                     cudaFuncAttributeMaxDynamicSharedMemorySize, (int)kNbrTileBytes);
-                if (e != cudaSuccess) return e;
-                configured = true;
-            }
-            spatial_prep_tiled_kernel<G, R><<<grid, block, kNbrTileBytes, st>>>(f, a);
-        } else {
-            spatial_prep_kernel<G, R><<<grid, block, 0, st>>>(f, a);
-        }
-    } break;
+    case kStageSpatial: spatial_prep_kernel<G, R><<<grid, block, 0, st>>>(f, a); break;
     case kStageCombine: {
         size_t P = (size_t)f.size[0] * f.size[1];
         combine_kernel<R><<<(unsigned)((P + 255) / 256), 256, 0, st>>>(f, L.pending, L.vis, L.direct_out, L.noisy_out);

@@ -369,15 +369,19 @@ extern "C" irt_status irt_server_run(irt_server* s, irt_server_stats* stats) {
             progressed = true;
         }
         if (rc) break;
-        // launches: every due session gets one frame per pass
+        // launches: every session gets its due frames, up to two in flight;
+        // a session behind schedule gets both back to back on its stream, so
+        // consecutive kernels reuse its scene and history in L2.
         now = seconds_since(t0);
         for (Active* a : active) {
-            if (a->inflight >= 2 || a->next_frame >= a->req.frames) continue;
-            double due = s->d.frame_rate > 0.f ? a->admitted + a->next_frame / (double)s->d.frame_rate : now;
-            if (due > now) continue;
-            rc = launch_frame(s, a, due);
+            while (a->inflight < 2 && a->next_frame < a->req.frames) {
+                double due = s->d.frame_rate > 0.f ? a->admitted + a->next_frame / (double)s->d.frame_rate : now;
+                if (due > now) break;
+                rc = launch_frame(s, a, due);
+                if (rc) break;
+                progressed = true;
+            }
             if (rc) break;
-            progressed = true;
         }
         now = seconds_since(t0);
         active_time += active.size() * (now - last_t);

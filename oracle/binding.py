@@ -154,7 +154,9 @@ class Oracle:
 
     def set_field_filter(self, linear: int):
         """0: point-sampled sample_field (common.wgsl:31-38); 1: the
-        reference's hardware-filtered variant (src/renderer.rs:277-286)."""
+        reference's hardware-filtered variant (src/renderer.rs:277-286) with
+        8-bit weights rounded to nearest; 2: the same with weights
+        truncated."""
         self.lib.oracle_set_field_filter(self.h_, int(linear))
 
     def set_rows(self, row0=0, row1=0xFFFFFFFF):

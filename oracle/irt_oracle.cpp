@@ -146,7 +146,8 @@ struct Scene {
     const irt_light* lights;
     const float* atlas;  // dequantised texels, x fastest
     uint32_t dims[3];
-    int field_linear = 0;  // 1: the reference's hardware-filtered sample_field
+    int field_linear = 0;  // 1: the reference's hardware-filtered sample_field (weights rounded to the
+                           // nearest 1/256), 2: the same with weights truncated to 1/256
 };
 
 struct GBuffer {  // F32 layout
@@ -410,10 +411,13 @@ struct Path {
     // filter is restated from the linear-filtering formula of the CUDA C++
     // Programming Guide ("Texture Fetching" appendix), which the device
     // sampler implements: x_B = x - 0.5, i = floor(x_B) and alpha = frac(x_B)
-    // held in 9-bit fixed point with 8 fractional bits (here rounded to the
-    // nearest 1/256), and the value is the sum over the 8 texels of
-    // (1 - alpha or alpha) products per axis, clamped to the atlas edge.
-    // Weighted in the same z, y, x order as sample_field.
+    // held in 9-bit fixed point with 8 fractional bits, and the value is the
+    // sum over the 8 texels of (1 - alpha or alpha) products per axis,
+    // clamped to the atlas edge.  Weighted in the same z, y, x order as
+    // sample_field.  The guide leaves the rounding of alpha and the
+    // arithmetic precision of the filter open: mode 1 rounds alpha to the
+    // nearest 1/256, mode 2 truncates it — two readings of the same
+    // documented filter, whose distance bounds what the documentation pins.
     T linear_field(const uint32_t origin[3], V3<T> q) const {
         const T qa[3] = {q.x, q.y, q.z};
         int64_t i0[3];
@@ -423,7 +427,8 @@ struct Path {
             const double xb = (double)x - 0.5;
             const double fl = std::floor(xb);
             i0[a] = (int64_t)fl;
-            alpha[a] = (T)(std::floor((xb - fl) * 256.0 + 0.5) / 256.0);
+            const double f256 = (xb - fl) * 256.0;
+            alpha[a] = (T)((sc.field_linear == 2 ? std::floor(f256) : std::floor(f256 + 0.5)) / 256.0);
         }
         auto at = [&](int a, int64_t i) {
             return (uint32_t)std::min<int64_t>(std::max<int64_t>(i, 0), (int64_t)sc.dims[a] - 1);
@@ -1255,7 +1260,8 @@ float oracle_quilez_step(float result, float h, float previous, float t, float k
 }
 
 // Field sampler of the session's march: 0 point-sampled trilinear
-// (common.wgsl:31-38), 1 the reference's filtered variant.
+// (common.wgsl:31-38), 1 the reference's filtered variant (weights rounded to
+// the nearest 1/256), 2 the filtered variant with truncated weights.
 void oracle_set_field_filter(void* s, int filter) { static_cast<State*>(s)->field_filter = filter; }
 
 // sample_field of one mesh at grid-space point q over an f32 atlas: the

@@ -81,7 +81,7 @@ def download_gbuffer(gt: dict, h: int, w: int, fmt: int) -> dict:
 class Lockstep:
     def __init__(self, wl: Workload, gbuffer_format=L.GBUFFER_F32, radiance_format=L.RADIANCE_F32, fused=1,
                  precision=0, moments_format=L.MOMENTS_F32, oracle_f16_storage=None, f64_witness=False,
-                 gpu_gbuffer=False, field_filter=L.FIELD_POINT, gpu_vpls=False):
+                 gpu_gbuffer=False, field_filter=L.FIELD_POINT, gpu_vpls=False, filter_witness=False):
         """precision 0: the oracle in f32 (the reference's arithmetic), 1: in
         f64.  oracle_f16_storage: round the oracle's radiance history to f16
         as the reference's Rgba16Float does (default: when the radiance
@@ -95,7 +95,12 @@ class Lockstep:
         field_filter: the SDF sampler of both sides (L.FIELD_LINEAR: the
         reference's hardware-filtered sample_field, emulated by the oracle).
         gpu_vpls: the VPL pools come from the CUDA generator
-        (irt_vpl_generate) and the oracle is given the pools it wrote."""
+        (irt_vpl_generate) and the oracle is given the pools it wrote.
+        filter_witness (with the filtered field sampler): also run an f32
+        oracle whose filter truncates its 8-bit weights instead of rounding
+        them, and report the CUDA outputs' error against it (`alt_<output>`)
+        and the primary oracle's (`filterfloor_<output>`): how far apart two
+        readings of the documented filter put the images."""
         self.wl = wl
         self.drv = FrameDriver(wl, gbuffer_format=gbuffer_format, radiance_format=radiance_format, fused=fused,
                                keep_candidates=True, moments_format=moments_format, gpu_gbuffer=gpu_gbuffer,
@@ -105,10 +110,13 @@ class Lockstep:
         args = (wl.width, wl.height, wl.settings.vpl_count, wl.settings.restir_max_history)
         self.orc = Oracle(*args, precision, oracle_f16_storage)
         self.witness = Oracle(*args, 1, False) if f64_witness else None
+        self.filter_witness = Oracle(*args, precision, oracle_f16_storage) if filter_witness else None
         self.drv.scene.set_field_filter(field_filter)
         for o in (self.orc, self.witness):
             if o is not None:
                 o.set_field_filter(field_filter)
+        if self.filter_witness is not None:
+            self.filter_witness.set_field_filter(2)
         self.fmt = gbuffer_format
         self.prev_vpls = None
         self.atlas = atlas_f32(wl)
@@ -116,7 +124,7 @@ class Lockstep:
     def frame(self, index: int, sync=True, debug=0):
         inputs = self.drv.inputs(index, debug)
         f, obj, nodes, lights, planes, vpls = inputs
-        orcs = [o for o in (self.orc, self.witness) if o is not None]
+        orcs = [o for o in (self.orc, self.witness, self.filter_witness) if o is not None]
         if sync and index > 0:
             for o in orcs:
                 sync_history(o, self.drv, index - 1)
@@ -153,13 +161,19 @@ class Lockstep:
             for k in ours:
                 out[f"f64_{k}"] = rel_l1(ours[k], w[k])
                 out[f"floor_{k}"] = rel_l1(ref[k], w[k])
+        if self.filter_witness is not None:
+            w = outputs(self.filter_witness, index)
+            for k in ours:
+                out[f"alt_{k}"] = rel_l1(ours[k], w[k])
+                out[f"filterfloor_{k}"] = rel_l1(ref[k], w[k])
         return out
 
     def close(self):
         self.drv.close()
         self.orc.close()
-        if self.witness is not None:
-            self.witness.close()
+        for o in (self.witness, self.filter_witness):
+            if o is not None:
+                o.close()
 
 
 def atlas_f32(wl: Workload) -> np.ndarray:
