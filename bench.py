@@ -303,19 +303,22 @@ def measured_peak():
         return 6650.0, "fallback"
 
 
-def ncu_traffic(kernel, workload):
-    """DRAM bytes (read + write) per launch of `kernel` on `workload` (e.g.
-    "1920x1200") from the committed ncu summary
-    profiles/<kernel>_kernel_<workload>.md (its line `dram_bytes_per_launch: N`),
-    or None when no capture of that workload is committed."""
+def ncu_figure(kernel, workload, key="dram_bytes_per_launch"):
+    """A figure of the committed ncu summary profiles/<kernel>_kernel_<workload>.md
+    (its line `<key>: N`, e.g. the DRAM bytes per launch of `kernel` on
+    "1920x1200"), or None when no capture of that workload is committed."""
     path = os.path.join(ROOT, "profiles", f"{kernel}_kernel_{workload}.md")
     try:
         for line in open(path):
-            if line.startswith("dram_bytes_per_launch:"):
+            if line.startswith(key + ":"):
                 return float(line.split(":", 1)[1].strip())
     except OSError:
         pass
     return None
+
+
+def ncu_traffic(kernel, workload):
+    return ncu_figure(kernel, workload)
 
 
 # ------------------------------------------------------------------ CPU legs
@@ -605,7 +608,12 @@ def ours(args):
                     "peak_source": "nominal FP32 SIMT peak (148 SMs x 128 lanes x 2 flops x 1.965 GHz); "
                                    "MEASURED_PEAKS.json holds no FP32 figure",
                     "flops_per_pixel": march_flops, "flops_model": FLOPS_PER, "counters_per_pixel": counters,
-                    "flops_note": "oracle work counters of a band of the same frame weighted by FLOPS_PER",
+                    "flops_note": "oracle work counters (the reference's BVH walk) of a band of the same frame "
+                                  "weighted by FLOPS_PER",
+                    "executed_flops_per_pixel": ncu_figure("march", "1920x1200", "executed_fp32_flops_per_pixel"),
+                    "executed_note": "FP32 operations the march executes per pixel (ncu thread-level FADD+FMUL+"
+                                     "2*FFMA at 480x300, profiles/march_kernel_1920x1200.md): the leaf-order "
+                                     "cache does the reference walk's work with fewer flops",
                     "hbm": hbm, "kernels": kernels}
     else:
         roofline = dict(bound="hbm", kernel=dominant, traffic=traffic, kernels=kernels, **hbm)
