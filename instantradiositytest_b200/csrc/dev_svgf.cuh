@@ -134,39 +134,6 @@ struct Sv {
         a.pixel_scale = distance(a.position, camera()) / (float)f.size[1];
         return a;
     }
-    // The factors of geometry_weight for a-trous, which multiplies in its
-    // luminance term: the normal weight `wn` and the sum of the exponents of
-    // the plane-distance and colour/parameter terms (`expo`, so the tap
-    // needs one exp for all three), with 1 / tolerance given per pixel.
-    // Returns false where the weight is zero (outside, or depth >= 1).
-    __device__ __forceinline__ bool geometry_terms(const Guide& a, int32_t qx, int32_t qy, float inv_tolerance,
-                                                   float& wn, float& expo) const {
-        if (!inside(qx, qy)) return false;
-        size_t q = idx(qx, qy);
-        if constexpr (kFeatures) {
-            if (c.feat) {
-                const float4 g = __ldg(c.guide + q);
-                if (g.w < 0.f) return false;  // depth >= 1
-                const float4 n = __ldg(c.feat + 2 * q), k = __ldg(c.feat + 2 * q + 1);
-                wn = pow64(wmax(dot(a.normal, xyz(n)), 0.f));
-                V3 dc = a.color - xyz(k);
-                float d0 = a.m0 - n.w, d1 = a.m1 - k.w;
-                expo = fabsf(dot(xyz(g) - a.position, a.normal)) * inv_tolerance + length(dc) * 8.f +
-                       sqrtf(d0 * d0 + d1 * d1) * 8.f;
-                return true;
-            }
-        }
-        float dq = c.g.d(q);
-        if (dq >= 1.f) return false;
-        V3 nq = c.g.n(q);
-        wn = pow64(wmax(dot(a.normal, nq), 0.f));
-        V3 wq = c.guide ? xyz(__ldg(c.guide + q)) : world(uvx(qx), uvy(qy), dq, f.inv_vp);
-        V3 dc = a.color - c.g.c(q);
-        float2 pm = c.g.pm(q);
-        float d0 = a.m0 - pm.x, d1 = a.m1 - pm.y;
-        expo = fabsf(dot(wq - a.position, a.normal)) * inv_tolerance + length(dc) * 8.f + sqrtf(d0 * d0 + d1 * d1) * 8.f;
-        return true;
-    }
     // svgf.wgsl:32-44
     __device__ __forceinline__ float geometry_weight(const Guide& a, int32_t qx, int32_t qy, float stride) const {
         if (!inside(qx, qy)) return 0.f;

@@ -98,17 +98,13 @@ __device__ __forceinline__ void atrous_body(const irt_frame& f, const SvgfCtx<G>
     V3 sum = V3{0.f, 0.f, 0.f};
     float total = 0.f, v = 0.f;
     float lc = luminance(V3{c4.x, c4.y, c4.z});
-    // Per pixel: 1 / phi and 1 / tolerance (svgf.wgsl:38); per tap one exp of
-    // the summed exponents of the plane, colour/parameter and luminance terms.
-    const float inv_phi = 1.f / phi;
-    const float inv_tolerance = 1.f / wmax(.0001f, a.pixel_scale * (float)step * .5f);
     auto tap = [&](int32_t xx, int32_t yy) {
         int32_t qx = x + xx * step, qy = y + yy * step;
-        float wn, expo;
-        if (!sv.geometry_terms(a, qx, qy, inv_tolerance, wn, expo) || wn <= 0.f) return;
+        float geom = sv.geometry_weight(a, qx, qy, (float)step);
+        if (geom <= 0.f) return;
         float4 smp = R::load(input, sv.idx(qx, qy));
-        float w = wavelet_kernel(xx) * wavelet_kernel(yy) * wn *
-                  __expf(-(expo + fabsf(luminance(V3{smp.x, smp.y, smp.z}) - lc) * inv_phi));
+        float w = wavelet_kernel(xx) * wavelet_kernel(yy) * geom *
+                  expf(-fabsf(luminance(V3{smp.x, smp.y, smp.z}) - lc) / phi);
         sum = sum + V3{smp.x, smp.y, smp.z} * w;
         v += smp.w * smp.w * w * w;
         total += w;
@@ -132,7 +128,7 @@ __device__ __forceinline__ void atrous_body(const irt_frame& f, const SvgfCtx<G>
 }
 
 template <class G, class R>
-__global__ void __launch_bounds__(256, 5) svgf_atrous_kernel(const __grid_constant__ irt_frame f, const __grid_constant__ SvgfCtx<G> c,
+__global__ void __launch_bounds__(256) svgf_atrous_kernel(const __grid_constant__ irt_frame f, const __grid_constant__ SvgfCtx<G> c,
                                                           const typename R::T* input, typename R::T* out,
                                                           typename R::T* out2, int32_t step) {
     atrous_body<G, R>(f, c, input, out, out2, step, blockIdx.x * blockDim.x + threadIdx.x,
