@@ -106,6 +106,13 @@ __device__ __forceinline__ void surface_terms(Surface& s, V3 camera) {
     s.f0 = V3{.04f * s.km + s.color.x * s.metal, .04f * s.km + s.color.y * s.metal, .04f * s.km + s.color.z * s.metal};
 }
 
+// Divisions of the shading functions below (brdf, direct, indirect): the
+// approximate divide (reciprocal and multiply, within 2 ulp; WGSL's own f32
+// division is specified to 2.5 ulp) instead of the IEEE sequence; every
+// denominator here is bounded below and far from the reciprocal's range
+// limit.  The visibility march keeps its own build's division.
+__device__ __forceinline__ float sdiv(float a, float b) { return __fdividef(a, b); }
+
 // common.wgsl:67-74 (GGX with Smith G1 terms plus Lambert, F0 = mix(.04, c, metal))
 // toward wi for the surface's view direction; (1 - vh)^5 by multiplication.
 __device__ __forceinline__ V3 brdf(const Surface& s, V3 wi) {
@@ -118,8 +125,8 @@ __device__ __forceinline__ V3 brdf(const Surface& s, V3 wi) {
     float vh = wmax(dot(wo, h), 0.f);
     const float a2 = s.a2;
     float q = nh * nh * (a2 - 1.f) + 1.f;
-    float d = a2 / (kPI * q * q);
-    float g1l = 2.f * nl / (nl + sqrtf(a2 + (1.f - a2) * nl * nl));
+    float d = sdiv(a2, kPI * q * q);
+    float g1l = sdiv(2.f * nl, nl + sqrtf(a2 + (1.f - a2) * nl * nl));
     const float km = s.km;
     const V3 f0 = s.f0;
     float x = 1.f - vh;
@@ -127,11 +134,11 @@ __device__ __forceinline__ V3 brdf(const Surface& s, V3 wi) {
     float p5 = x2 * x2 * x;
     V3 fr = V3{f0.x + (1.f - f0.x) * p5, f0.y + (1.f - f0.y) * p5, f0.z + (1.f - f0.z) * p5};
     float den = wmax(4.f * nv * nl, .00001f);
-    float spec = d * s.g1v * g1l / den;
+    float spec = sdiv(d * s.g1v * g1l, den);
     V3 out;
-    out.x = (1.f - fr.x) * km * s.color.x / kPI + fr.x * spec;
-    out.y = (1.f - fr.y) * km * s.color.y / kPI + fr.y * spec;
-    out.z = (1.f - fr.z) * km * s.color.z / kPI + fr.z * spec;
+    out.x = sdiv((1.f - fr.x) * km * s.color.x, kPI) + fr.x * spec;
+    out.y = sdiv((1.f - fr.y) * km * s.color.y, kPI) + fr.y * spec;
+    out.z = sdiv((1.f - fr.z) * km * s.color.z, kPI) + fr.z * spec;
     return out;
 }
 
@@ -168,24 +175,25 @@ __device__ __forceinline__ DLight prepare_light(const irt_light& l) {
 __device__ __forceinline__ V3 direct(const Surface& s, const DLight& l) {
     V3 delta = xyz(l.ps) - s.p;
     float r2 = wmax(dot(delta, delta), .0001f);
-    V3 wi = delta * (1.f / sqrtf(r2));
+    V3 wi = delta * sdiv(1.f, sqrtf(r2));
     if (l.ct.w > 0.5f && dot(-wi, xyz(l.da)) < l.da.w) return V3{0.f, 0.f, 0.f};
     V3 b = brdf(s, wi);
     float nl = wmax(dot(s.n, wi), 0.f);
     float st = l.ps.w;
-    return V3{b.x * nl * l.ct.x * st / r2, b.y * nl * l.ct.y * st / r2, b.z * nl * l.ct.z * st / r2};
+    return V3{sdiv(b.x * nl * l.ct.x * st, r2), sdiv(b.y * nl * l.ct.y * st, r2), sdiv(b.z * nl * l.ct.z * st, r2)};
 }
 
 // common.wgsl:80-83
 __device__ __forceinline__ V3 indirect(const Surface& s, const DVpl& v) {
     V3 delta = xyz(v.pos) - s.p;
     float r2 = wmax(dot(delta, delta), .0025f);
-    V3 wi = delta * (1.f / sqrtf(r2));
+    V3 wi = delta * sdiv(1.f, sqrtf(r2));
     V3 b = brdf(s, wi);
     float nl = wmax(dot(s.n, wi), 0.f);
     float ne = wmax(dot(xyz(v.nrm), -wi), 0.f);
     float den = 4.f * kPI * r2;
-    return V3{b.x * nl * ne * v.flux.x / den, b.y * nl * ne * v.flux.y / den, b.z * nl * ne * v.flux.z / den};
+    return V3{sdiv(b.x * nl * ne * v.flux.x, den), sdiv(b.y * nl * ne * v.flux.y, den),
+              sdiv(b.z * nl * ne * v.flux.z, den)};
 }
 
 // ------------------------------------------------------------------ reservoirs

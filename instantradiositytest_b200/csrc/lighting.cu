@@ -42,12 +42,23 @@ struct LightArgs {
     const float4* feat;       // decoded (normal, rough), (colour, metal) per pixel, or null
 };
 
+// Scenes of at most kLightTable lights: the reuse pass evaluates every
+// light's target (luminance of the unshadowed direct term) once per pixel,
+// all independent, into a per-thread column of shared memory; the RIS loop
+// and the temporal merge then read their light's entry.  Each entry is the
+// same function of the same operands as the per-candidate evaluation, so
+// the bits are too; what changes is that the 8 evaluations no longer wait
+// on each other through the random stream.
+constexpr uint32_t kLightTable = 8;
+constexpr uint32_t kLightTableStride = 256;  // threads per block of the lighting kernels
+
 template <class G>
 struct Px {
     const irt_frame& f;
     const LightArgs<G>& a;
     uint32_t x, y;
     size_t id;
+    const float* ltab = nullptr;  // light j's target at ltab[j * kLightTableStride], or null
     __device__ __forceinline__ Px(const irt_frame& fr, const LightArgs<G>& ar, uint32_t px, uint32_t py)
         : f(fr), a(ar), x(px), y(py), id((size_t)py * fr.size[0] + px) {}
 
@@ -148,7 +159,7 @@ struct Px {
             float pdf = 1.f / (float)f.counts[0];
             for (uint32_t i = 0; i < f.restir[0]; i++) {
                 uint32_t lid = min(to_u32(rnd(rng) * (float)f.counts[0]), f.counts[0] - 1u);
-                float target = luminance(direct(s, load_light(a.sc.lights, lid)));
+                float target = ltab ? ltab[lid * kLightTableStride] : luminance(direct(s, load_light(a.sc.lights, lid)));
                 res_add(r, lid, f.size[2], target, pdf, target / pdf, 1u, 0u, rng);
             }
         }
@@ -175,7 +186,8 @@ struct Px {
         Res previous = cap(res_load(a.dres[2], (size_t)qy * f.size[0] + (size_t)qx), to_u32(f.rr[2]) * f.restir[0]);
         if (previous.generation == f.size[3] && previous.target > 0.f && previous.id < f.counts[0] &&
             previous.age < to_u32(f.rr[2])) {
-            float target = luminance(direct(s, load_light(a.sc.lights, previous.id)));
+            float target = ltab ? ltab[previous.id * kLightTableStride]
+                                : luminance(direct(s, load_light(a.sc.lights, previous.id)));
             res_add(r, previous.id, previous.source, target, previous.pdf,
                     target * normalization(previous) * (float)previous.count, previous.count, previous.age + 1u, rng);
         }
@@ -287,6 +299,15 @@ __device__ __forceinline__ void reuse_body(const irt_frame& f, const LightArgs<G
     bool ok = px.valid();
     Surface s;
     if (ok) s = px.surface();
+    __shared__ float ltab[kLightTable * kLightTableStride];
+    const uint32_t t = threadIdx.y * blockDim.x + threadIdx.x;
+    if (ok && f.counts[0] <= kLightTable && blockDim.x * blockDim.y == kLightTableStride) {
+        const uint32_t n = f.counts[0];
+#pragma unroll
+        for (uint32_t j = 0; j < kLightTable; j++)
+            if (j < n) ltab[j * kLightTableStride + t] = luminance(direct(s, load_light(a.sc.lights, j)));
+        px.ltab = ltab + t;
+    }
     Res rd = px.candidates_direct(ok, s);
     Res ri = px.candidates_indirect(ok, s);
     if (keep_candidates) {
