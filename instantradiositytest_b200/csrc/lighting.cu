@@ -51,15 +51,6 @@ struct LightArgs {
 // on each other through the random stream.
 constexpr uint32_t kLightTable = 8;
 constexpr uint32_t kLightTableStride = 256;  // threads per block of the lighting kernels
-// The VPL candidates (lighting.wgsl:59-65) up to kVplAhead of them: candidate
-// i reads its VPL id from draw p_i of its random stream, p_0 = 0 and
-// p_{i+1} = p_i + 1, or + 2 after an accepted weight (add() draws the
-// selection number then), so p_i lies in [i, 2i].  The reuse pass draws the
-// stream's first 2n numbers, evaluates the target of the VPL every draw in
-// [0, 2n-2] names — independent evaluations instead of a chain — and then
-// runs the reservoir additions in order from the two tables: the same draws
-// and targets in the same order, so the same reservoir.
-constexpr uint32_t kVplAhead = 8;
 
 template <class G>
 struct Px {
@@ -174,47 +165,6 @@ struct Px {
         }
         return r;
     }
-    // lighting.wgsl:59-65 from the tables of draws (draws[k * stride]) and
-    // targets (targets[k * stride]); see kVplAhead.
-    __device__ __forceinline__ Res candidates_indirect_ahead(bool ok, const Surface& s, float* draws,
-                                                             float* targets) const {
-        Res r = res_empty(f);
-        uint32_t rng = seed((uint32_t)id, 13u, f.size[2]);
-        if (!ok) return r;
-        const uint32_t n = f.restir[1], count = f.counts[1];
-        const float pdf = 1.f / (float)count;
-#pragma unroll
-        for (uint32_t k = 0; k < 2 * kVplAhead; k++)
-            if (k < 2 * n) draws[k * kLightTableStride] = rnd(rng);
-#pragma unroll
-        for (uint32_t k = 0; k + 1 < 2 * kVplAhead; k++)
-            if (k + 1 < 2 * n) {
-                const uint32_t vid = min(to_u32(draws[k * kLightTableStride] * (float)count), count - 1u);
-                targets[k * kLightTableStride] = luminance(indirect(s, load_vpl(a.cur, vid)));
-            }
-        uint32_t p = 0;
-        for (uint32_t i = 0; i < n; i++) {
-            const uint32_t vid = min(to_u32(draws[p * kLightTableStride] * (float)count), count - 1u);
-            const float target = targets[p * kLightTableStride];
-            const float weight = target / pdf;
-            // res_add with its selection draw read from the table
-            r.count += 1u;
-            if (weight <= 0.f || weight > 1e30f) {
-                p += 1u;
-                continue;
-            }
-            r.sum += weight;
-            if (draws[(p + 1) * kLightTableStride] * r.sum < weight) {
-                r.id = vid;
-                r.source = f.size[2];
-                r.target = target;
-                r.pdf = pdf;
-                r.age = 0u;
-            }
-            p += 2u;
-        }
-        return r;
-    }
     // lighting.wgsl:59-65
     __device__ __forceinline__ Res candidates_indirect(bool ok, const Surface& s) const {
         Res r = res_empty(f);
@@ -269,8 +219,7 @@ struct Px {
                 Res previous = res_load(in, (size_t)qy * f.size[0] + (size_t)qx);
                 if (Dom == 0) {
                     if (previous.target > 0.f && index_ok(a.sc.error, previous.id, f.counts[0])) {
-                        float target = ltab ? ltab[previous.id * kLightTableStride]
-                                            : luminance(direct(s, load_light(a.sc.lights, previous.id)));
+                        float target = luminance(direct(s, load_light(a.sc.lights, previous.id)));
                         res_add(r, previous.id, previous.source, target, previous.pdf,
                                 target * normalization(previous) * (float)previous.count, previous.count, previous.age,
                                 rng);
@@ -341,20 +290,6 @@ __global__ void prepare_lights_kernel(const irt_light* lights, uint32_t n, irt_l
     o[2] = l.ct;
 }
 
-// The per-thread column of light targets (kLightTable), when the scene has
-// few enough lights and the block the table's thread count.
-template <class G>
-__device__ __forceinline__ void fill_light_table(const irt_frame& f, const LightArgs<G>& a, const Surface& s,
-                                                 float* ltab, Px<G>& px) {
-    const uint32_t t = threadIdx.y * blockDim.x + threadIdx.x;
-    if (f.counts[0] > kLightTable || blockDim.x * blockDim.y != kLightTableStride) return;
-    const uint32_t n = f.counts[0];
-#pragma unroll
-    for (uint32_t j = 0; j < kLightTable; j++)
-        if (j < n) ltab[j * kLightTableStride + t] = luminance(direct(s, load_light(a.sc.lights, j)));
-    px.ltab = ltab + t;
-}
-
 // ---------------------------------------------------------------- fused kernels
 template <class G>
 __device__ __forceinline__ void reuse_body(const irt_frame& f, const LightArgs<G>& a, int keep_candidates, uint32_t x,
@@ -365,14 +300,16 @@ __device__ __forceinline__ void reuse_body(const irt_frame& f, const LightArgs<G
     Surface s;
     if (ok) s = px.surface();
     __shared__ float ltab[kLightTable * kLightTableStride];
-    if (ok) fill_light_table(f, a, s, ltab, px);
-    Res rd = px.candidates_direct(ok, s);
-    __shared__ float vdraws[2 * kVplAhead * kLightTableStride];
-    __shared__ float vtargets[(2 * kVplAhead - 1) * kLightTableStride];
     const uint32_t t = threadIdx.y * blockDim.x + threadIdx.x;
-    Res ri = f.restir[1] <= kVplAhead && blockDim.x * blockDim.y == kLightTableStride
-                 ? px.candidates_indirect_ahead(ok, s, vdraws + t, vtargets + t)
-                 : px.candidates_indirect(ok, s);
+    if (ok && f.counts[0] <= kLightTable && blockDim.x * blockDim.y == kLightTableStride) {
+        const uint32_t n = f.counts[0];
+#pragma unroll
+        for (uint32_t j = 0; j < kLightTable; j++)
+            if (j < n) ltab[j * kLightTableStride + t] = luminance(direct(s, load_light(a.sc.lights, j)));
+        px.ltab = ltab + t;
+    }
+    Res rd = px.candidates_direct(ok, s);
+    Res ri = px.candidates_indirect(ok, s);
     if (keep_candidates) {
         res_store(a.dres[0], px.id, rd);
         res_store(a.ires[0], px.id, ri);
@@ -442,8 +379,6 @@ __device__ __forceinline__ void spatial_prep_body(const irt_frame& f, const Ligh
         bool ok = px.valid();
         Surface s;
         if (ok) s = px.surface();
-        __shared__ float ltab[kLightTable * kLightTableStride];
-        if (ok) fill_light_table(f, a, s, ltab, px);
         Res rd = px.template spatial<0>(res_load(a.dres[1], px.id), ok, s);
         res_store(a.dres[2], px.id, rd);
         Res ri = px.template spatial<1>(res_load(a.ires[1], px.id), ok, s);
