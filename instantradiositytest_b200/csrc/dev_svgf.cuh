@@ -134,58 +134,36 @@ struct Sv {
         a.pixel_scale = distance(a.position, camera()) / (float)f.size[1];
         return a;
     }
-    // A neighbour's edge-stopping inputs (svgf.wgsl:32-44), loaded once so
-    // that pixels sharing the neighbour weight it from the same registers;
-    // ok = false outside the image or at depth >= 1 (weight 0).
-    struct Tap {
-        V3 position, normal, color;
-        float m0, m1;
-        bool ok;
-    };
-    __device__ __forceinline__ Tap tap_at(int32_t qx, int32_t qy) const {
-        Tap t;
-        t.ok = false;
-        if (!inside(qx, qy)) return t;
+    // svgf.wgsl:32-44
+    __device__ __forceinline__ float geometry_weight(const Guide& a, int32_t qx, int32_t qy, float stride) const {
+        if (!inside(qx, qy)) return 0.f;
         size_t q = idx(qx, qy);
         if constexpr (kFeatures) {
             if (c.feat) {
                 const float4 g = __ldg(c.guide + q);
-                if (g.w < 0.f) return t;  // depth >= 1
+                if (g.w < 0.f) return 0.f;  // depth >= 1
                 const float4 n = __ldg(c.feat + 2 * q), k = __ldg(c.feat + 2 * q + 1);
-                t.position = xyz(g);
-                t.normal = xyz(n);
-                t.color = xyz(k);
-                t.m0 = n.w;
-                t.m1 = k.w;
-                t.ok = true;
-                return t;
+                float wn = pow64(wmax(dot(a.normal, xyz(n)), 0.f));
+                float tolerance = wmax(.0001f, a.pixel_scale * stride * .5f);
+                float wz = expf(-fabsf(dot(xyz(g) - a.position, a.normal)) / tolerance);
+                V3 dc = a.color - xyz(k);
+                float d0 = a.m0 - n.w, d1 = a.m1 - k.w;
+                float wc = expf(-length(dc) * 8.f - sqrtf(d0 * d0 + d1 * d1) * 8.f);
+                return wn * wz * wc;
             }
         }
         float dq = c.g.d(q);
-        if (dq >= 1.f) return t;
-        t.normal = c.g.n(q);
-        t.position = c.guide ? xyz(__ldg(c.guide + q)) : world(uvx(qx), uvy(qy), dq, f.inv_vp);
-        t.color = c.g.c(q);
-        float2 pm = c.g.pm(q);
-        t.m0 = pm.x;
-        t.m1 = pm.y;
-        t.ok = true;
-        return t;
-    }
-    // svgf.wgsl:32-44: normal^64 x exp(-plane distance / tolerance) x
-    // exp(-8|colour difference| - 8|parameter difference|).
-    __device__ __forceinline__ float tap_weight(const Guide& a, const Tap& t, float stride) const {
-        if (!t.ok) return 0.f;
-        float wn = pow64(wmax(dot(a.normal, t.normal), 0.f));
+        if (dq >= 1.f) return 0.f;
+        V3 nq = c.g.n(q);
+        float wn = pow64(wmax(dot(a.normal, nq), 0.f));
+        V3 wq = c.guide ? xyz(__ldg(c.guide + q)) : world(uvx(qx), uvy(qy), dq, f.inv_vp);
         float tolerance = wmax(.0001f, a.pixel_scale * stride * .5f);
-        float wz = expf(-fabsf(dot(t.position - a.position, a.normal)) / tolerance);
-        V3 dc = a.color - t.color;
-        float d0 = a.m0 - t.m0, d1 = a.m1 - t.m1;
+        float wz = expf(-fabsf(dot(wq - a.position, a.normal)) / tolerance);
+        V3 dc = a.color - c.g.c(q);
+        float2 pm = c.g.pm(q);
+        float d0 = a.m0 - pm.x, d1 = a.m1 - pm.y;
         float wc = expf(-length(dc) * 8.f - sqrtf(d0 * d0 + d1 * d1) * 8.f);
         return wn * wz * wc;
-    }
-    __device__ __forceinline__ float geometry_weight(const Guide& a, int32_t qx, int32_t qy, float stride) const {
-        return tap_weight(a, tap_at(qx, qy), stride);
     }
 };
 

@@ -67,29 +67,22 @@ __device__ __forceinline__ float wavelet_kernel(int32_t x) {
     return 1.f / 6.f;
 }
 
-// One pixel's a-trous state (svgf.wgsl:91-110): its guide, the luminance
-// and phi of its weights, and the weighted sums.
-struct AtrousAcc {
-    Guide a;
-    float lc, phi;
-    V3 sum;
-    float total, v;
-};
-
-// The pixel's set-up: false (and the input copied through) at depth >= 1.
+// svgf.wgsl:91-110; `out2` (optional) receives a second copy of the result.
 template <class G, class R>
-__device__ __forceinline__ bool atrous_begin(const Sv<G>& sv, const SvgfCtx<G>& c, const typename R::T* input,
-                                             typename R::T* out, typename R::T* out2, int32_t x, int32_t y,
-                                             AtrousAcc& p) {
+__device__ __forceinline__ void atrous_body(const irt_frame& f, const SvgfCtx<G>& c, const typename R::T* input,
+                                            typename R::T* out, typename R::T* out2, int32_t step, int32_t x,
+                                            int32_t y) {
+    Sv<G> sv(f, c);
+    if (x >= sv.W || y >= sv.H) return;
     size_t i = sv.idx(x, y);
     float4 c4 = R::load(input, i);
     if (c.g.d(i) >= 1.f) {
         R::store(out, i, c4);
         if (out2) R::store(out2, i, c4);
-        return false;
+        return;
     }
     float variance = 0.f, guide_weight = 0.f;
-    p.a = sv.guide(x, y);
+    Guide a = sv.guide(x, y);
 #pragma unroll
     for (int32_t yy = -1; yy <= 1; yy++)
 #pragma unroll
@@ -101,49 +94,20 @@ __device__ __forceinline__ bool atrous_begin(const Sv<G>& sv, const SvgfCtx<G>& 
             variance += s * s * w;
             guide_weight += w;
         }
-    p.phi = 4.f * sqrtf(variance / wmax(guide_weight, .00001f)) + .0001f;
-    p.sum = V3{0.f, 0.f, 0.f};
-    p.total = 0.f;
-    p.v = 0.f;
-    p.lc = luminance(V3{c4.x, c4.y, c4.z});
-    return true;
-}
-
-// Tap (xx, yy) of the 5x5 window, with its inputs and radiance loaded.
-template <class G>
-__device__ __forceinline__ void atrous_add(const Sv<G>& sv, AtrousAcc& p, const typename Sv<G>::Tap& t, float4 smp,
-                                           int32_t xx, int32_t yy, float stride) {
-    float geom = sv.tap_weight(p.a, t, stride);
-    if (geom <= 0.f) return;
-    float w = wavelet_kernel(xx) * wavelet_kernel(yy) * geom *
-              expf(-fabsf(luminance(V3{smp.x, smp.y, smp.z}) - p.lc) / p.phi);
-    p.sum = p.sum + V3{smp.x, smp.y, smp.z} * w;
-    p.v += smp.w * smp.w * w * w;
-    p.total += w;
-}
-
-template <class R>
-__device__ __forceinline__ void atrous_end(const AtrousAcc& p, size_t i, typename R::T* out, typename R::T* out2) {
-    float dn = wmax(p.total, .00001f);
-    float4 o = make_float4(p.sum.x / dn, p.sum.y / dn, p.sum.z / dn, wmin(sqrtf(p.v) / dn, 65000.f));
-    R::store(out, i, o);
-    if (out2) R::store(out2, i, o);
-}
-
-// svgf.wgsl:91-110; `out2` (optional) receives a second copy of the result.
-template <class G, class R>
-__device__ __forceinline__ void atrous_body(const irt_frame& f, const SvgfCtx<G>& c, const typename R::T* input,
-                                            typename R::T* out, typename R::T* out2, int32_t step, int32_t x,
-                                            int32_t y) {
-    Sv<G> sv(f, c);
-    if (x >= sv.W || y >= sv.H) return;
-    AtrousAcc p;
-    if (!atrous_begin<G, R>(sv, c, input, out, out2, x, y, p)) return;
+    float phi = 4.f * sqrtf(variance / wmax(guide_weight, .00001f)) + .0001f;
+    V3 sum = V3{0.f, 0.f, 0.f};
+    float total = 0.f, v = 0.f;
+    float lc = luminance(V3{c4.x, c4.y, c4.z});
     auto tap = [&](int32_t xx, int32_t yy) {
         int32_t qx = x + xx * step, qy = y + yy * step;
-        const typename Sv<G>::Tap t = sv.tap_at(qx, qy);
-        if (!t.ok) return;
-        atrous_add(sv, p, t, R::load(input, sv.idx(qx, qy)), xx, yy, (float)step);
+        float geom = sv.geometry_weight(a, qx, qy, (float)step);
+        if (geom <= 0.f) return;
+        float4 smp = R::load(input, sv.idx(qx, qy));
+        float w = wavelet_kernel(xx) * wavelet_kernel(yy) * geom *
+                  expf(-fabsf(luminance(V3{smp.x, smp.y, smp.z}) - lc) / phi);
+        sum = sum + V3{smp.x, smp.y, smp.z} * w;
+        v += smp.w * smp.w * w * w;
+        total += w;
     };
     // Taps in row order.  With feature records (three 128-bit loads a tap)
     // a row's five taps are unrolled so their loads issue together (a-trous
@@ -157,49 +121,10 @@ __device__ __forceinline__ void atrous_body(const irt_frame& f, const SvgfCtx<G>
         for (int32_t yy = -2; yy <= 2; yy++)
             for (int32_t xx = -2; xx <= 2; xx++) tap(xx, yy);
     }
-    atrous_end<R>(p, sv.idx(x, y), out, out2);
-}
-
-// Two pixels of a column `step` rows apart per thread, (x, ya) and
-// (x, ya + step): their 5x5 windows share four rows, so the thread loads the
-// 30 taps of rows ya - 2 step .. ya + 3 step once for both instead of 50.
-// Each pixel adds its taps in the same order with the same operations as
-// atrous_body, so its result is the same.  Pair row j covers rows
-// (j / step) * 2 step + j % step and that + step.
-template <class G, class R>
-__device__ __forceinline__ void atrous_pair_body(const irt_frame& f, const SvgfCtx<G>& c, const typename R::T* input,
-                                                 typename R::T* out, typename R::T* out2, int32_t step, int32_t x,
-                                                 int32_t j) {
-    Sv<G> sv(f, c);
-    const int32_t ya = (j / step) * 2 * step + j % step, yb = ya + step;
-    if (x >= sv.W || ya >= sv.H) return;
-    AtrousAcc pa, pb;
-    const bool a_on = atrous_begin<G, R>(sv, c, input, out, out2, x, ya, pa);
-    const bool b_on = yb < sv.H && atrous_begin<G, R>(sv, c, input, out, out2, x, yb, pb);
-    if (!a_on && !b_on) return;
-    for (int32_t dy = -2; dy <= 3; dy++) {
-        if ((dy == 3 && !b_on) || (dy == -2 && !a_on)) continue;
-        const int32_t qy = ya + dy * step;
-        for (int32_t xx = -2; xx <= 2; xx++) {
-            const int32_t qx = x + xx * step;
-            const typename Sv<G>::Tap t = sv.tap_at(qx, qy);
-            if (!t.ok) continue;
-            const float4 smp = R::load(input, sv.idx(qx, qy));
-            if (a_on && dy <= 2) atrous_add(sv, pa, t, smp, xx, dy, (float)step);
-            if (b_on && dy >= -1) atrous_add(sv, pb, t, smp, xx, dy - 1, (float)step);
-        }
-    }
-    if (a_on) atrous_end<R>(pa, sv.idx(x, ya), out, out2);
-    if (b_on) atrous_end<R>(pb, sv.idx(x, yb), out, out2);
-}
-
-template <class G, class R>
-__global__ void __launch_bounds__(256, 4) svgf_atrous_pair_kernel(const __grid_constant__ irt_frame f,
-                                                               const __grid_constant__ SvgfCtx<G> c,
-                                                               const typename R::T* input, typename R::T* out,
-                                                               typename R::T* out2, int32_t step) {
-    atrous_pair_body<G, R>(f, c, input, out, out2, step, blockIdx.x * blockDim.x + threadIdx.x,
-                           blockIdx.y * blockDim.y + threadIdx.y);
+    float dn = wmax(total, .00001f);
+    float4 o = make_float4(sum.x / dn, sum.y / dn, sum.z / dn, wmin(sqrtf(v) / dn, 65000.f));
+    R::store(out, i, o);
+    if (out2) R::store(out2, i, o);
 }
 
 template <class G, class R>
@@ -252,13 +177,8 @@ static cudaError_t spatial_typed(const SvgfLaunch& L, int stage, cudaStream_t st
     if (stage == 1)
         svgf_variance_kernel<G, R, M><<<grid, block, 0, st>>>(f, c, (const T*)L.in,
                                                               (const typename M::T*)L.moments_in, (T*)L.out);
-    else if (stage == 2) {
-        // pair rows: ceil(H / (2 step)) groups of `step` rows
-        const uint32_t s2 = (uint32_t)L.step;
-        const uint32_t pair_rows = (f.size[1] + 2 * s2 - 1) / (2 * s2) * s2;
-        dim3 pgrid((f.size[0] + 31) / 32, (pair_rows + 7) / 8);
-        svgf_atrous_pair_kernel<G, R><<<pgrid, block, 0, st>>>(f, c, (const T*)L.in, (T*)L.out, (T*)L.out2, L.step);
-    }
+    else if (stage == 2)
+        svgf_atrous_kernel<G, R><<<grid, block, 0, st>>>(f, c, (const T*)L.in, (T*)L.out, (T*)L.out2, L.step);
     else
         return cudaErrorInvalidValue;
     return cudaGetLastError();
