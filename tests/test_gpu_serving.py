@@ -112,7 +112,7 @@ def test_served_session_against_the_oracle(cuda, scenes):
     ls = Lockstep(wl, gpu_gbuffer=True, gpu_vpls=True)
     rows = [ls.frame(i) for i in range(frames)]
     mine = ls.drv.session.buffer(L.BUF_FILTERED, torch.uint8).cpu().numpy()
-    ref = outputs(ls.orc, frames - 1)["filtered"]
+    ref = outputs(ls.orc, frames - 1)["filtered"].copy()  # a view of the oracle's buffer until close()
     ls.close()
     worst = {k: (min(r[k] for r in rows) if k.startswith("select") else max(r[k] for r in rows)) for k in rows[0]}
     print("served session lockstep", worst)
