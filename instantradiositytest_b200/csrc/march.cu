@@ -203,7 +203,7 @@ __device__ __forceinline__ void march_reset(MarchState& m) {
     m.step = 0;
 }
 
-__global__ void __launch_bounds__(128, 10) march_kernel(const __grid_constant__ irt_frame f, const DevScene sc,
+__global__ void __launch_bounds__(128, 8) march_kernel(const __grid_constant__ irt_frame f, const DevScene sc,
                                                     const float4* __restrict__ march_scene, uint32_t scene_vec4,
                                                     const Grid grid, const RayRecord* __restrict__ rays,
                                                     uint32_t* counters, float* __restrict__ vis) {
@@ -227,16 +227,8 @@ __global__ void __launch_bounds__(128, 10) march_kernel(const __grid_constant__ 
     // A lane keeps its ray's index and re-reads the record's target, endpoint
     // normal and output slot where a step needs them (L1/L2 hits), which
     // keeps fewer values live across the loop.
-    struct RayState {
-        MarchState m;
-        uint32_t phase, ridx;
-    };
-    RayState& rs = reinterpret_cast<RayState*>(smem + scene_vec4)[threadIdx.x];
-    uint32_t& phase = rs.phase;
-    uint32_t& ridx = rs.ridx;
-    MarchState& m = rs.m;
-    phase = kClear;
-    ridx = 0;
+    uint32_t phase = kClear, ridx = 0;
+    MarchState m;
     march_reset(m);
     Query qy;
     qy.cur = kQueryDone;
@@ -418,10 +410,9 @@ cudaError_t IRT_MARCH_LAUNCH(const MarchLaunch& M, cudaStream_t st) {
     cudaGetDevice(&device);
     if (smem != configured_smem || device != configured_device) {
         configured_device = device;
-        cudaError_t e = cudaFuncSetAttribute(march_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                             (int)(smem + 128 * 64));
+        cudaError_t e = cudaFuncSetAttribute(march_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
         if (e != cudaSuccess) return e;
-        e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&blocks_per_sm, march_kernel, 128, smem + 128 * 64);
+        e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&blocks_per_sm, march_kernel, 128, smem);
         if (e != cudaSuccess) return e;
         if (blocks_per_sm < 1) return cudaErrorInvalidConfiguration;
         configured_smem = smem;
@@ -444,7 +435,7 @@ cudaError_t IRT_MARCH_LAUNCH(const MarchLaunch& M, cudaStream_t st) {
     g.ix = M.grid_inv[0];
     g.iy = M.grid_inv[1];
     g.iz = M.grid_inv[2];
-    march_kernel<<<M.num_sms * blocks_per_sm, 128, smem + 128 * 64, st>>>(*M.frame, sc, M.march_scene, smem / 16, g, M.rays,
+    march_kernel<<<M.num_sms * blocks_per_sm, 128, smem, st>>>(*M.frame, sc, M.march_scene, smem / 16, g, M.rays,
                                                                 M.ray_counters, M.vis);
     return cudaGetLastError();
 }
