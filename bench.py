@@ -994,6 +994,9 @@ def batched(args):
 def main():
     args = parse()
     if args.impl == "reference":
+        # The reference arm runs the oracle; its inputs come from the host-only
+        # library (generator and CPU producers), so no CUDA code is loaded.
+        os.environ["IRT_LIBRARY"] = "host"
         reference_arm(args)
     elif args.config == 4:
         serve(args)

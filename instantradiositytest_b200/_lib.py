@@ -4,7 +4,10 @@ The shared library is built in-tree (``make -C instantradiositytest_b200``) and
 loaded from this directory.  There is no fallback: importing this module
 without the library raises ``ImportError``.  With IRT_LIBRARY=checked in the
 environment the checked build (libirt_checked.so, the same C-ABI with every
-data-dependent index tested in the kernels) is loaded instead.
+data-dependent index tested in the kernels) is loaded instead; with
+IRT_LIBRARY=host the host-only library (libirt_host.so: workload generator,
+CPU producers, scene loader, host logic — no CUDA code), which binds only
+the functions it has.
 """
 from __future__ import annotations
 
@@ -15,7 +18,10 @@ import numpy as np
 
 _HERE = os.path.dirname(os.path.abspath(__file__))
 CHECKED_LIB_PATH = os.path.join(_HERE, "libirt_checked.so")
-LIB_PATH = CHECKED_LIB_PATH if os.environ.get("IRT_LIBRARY") == "checked" else os.path.join(_HERE, "libirt.so")
+HOST_LIB_PATH = os.path.join(_HERE, "libirt_host.so")
+LIB_PATH = {"checked": CHECKED_LIB_PATH, "host": HOST_LIB_PATH}.get(os.environ.get("IRT_LIBRARY", ""),
+                                                                   os.path.join(_HERE, "libirt.so"))
+HOST_ONLY = LIB_PATH == HOST_LIB_PATH
 
 IRT_OK = 0
 IRT_E_INVALID = -1
@@ -242,6 +248,8 @@ def _load():
             "there is no CPU fallback")
     lib = C.CDLL(LIB_PATH)
     for name, (res, args) in _PROTOS.items():
+        if HOST_ONLY and not hasattr(lib, name):
+            continue  # a device entry point the host-only library does not have
         fn = getattr(lib, name)
         fn.restype = res
         fn.argtypes = args

@@ -1046,14 +1046,5 @@ irt_status irt_session_reservoirs(irt_session* s, int32_t domain, int32_t k, voi
     return IRT_OK;
 }
 
-void irt_workload_destroy(irt_workload* wl) {
-    if (!wl) return;
-    if (wl->w.dev_prims || wl->w.dev_nodes || wl->w.dev_tris) {
-        DeviceGuard g(wl->w.dev_prims_device);
-        for (void* p : {wl->w.dev_prims, wl->w.dev_nodes, wl->w.dev_tris})
-            if (p) cudaFree(p);
-    }
-    delete wl;
-}
 
 }  // extern "C"

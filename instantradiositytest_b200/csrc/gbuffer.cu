@@ -103,6 +103,18 @@ __global__ void gbuffer_kernel(const __grid_constant__ irt_frame f, const irt::P
 // scenes: built once and kept with the workload), with the triangle
 // hierarchies of loaded meshes concatenated into shared node and triangle
 // tables.
+// Frees a workload's device primitive tables (Workload::release_device).
+static void release_prims(irt::Workload& w) {
+    int prev = -1;
+    cudaGetDevice(&prev);
+    const bool other = w.dev_prims_device >= 0 && prev != w.dev_prims_device;
+    if (other) cudaSetDevice(w.dev_prims_device);
+    for (void* p : {w.dev_prims, w.dev_nodes, w.dev_tris})
+        if (p) cudaFree(p);
+    w.dev_prims = w.dev_nodes = w.dev_tris = nullptr;
+    if (other && prev >= 0) cudaSetDevice(prev);
+}
+
 cudaError_t irt_workload_prims(const irt_workload* wl_c, irt::PrimTable* out) {
     irt_workload* wl = const_cast<irt_workload*>(wl_c);
     irt::Workload& w = wl->w;
@@ -163,6 +175,7 @@ cudaError_t irt_workload_prims(const irt_workload* wl_c, irt::PrimTable* out) {
             *p = nullptr;
         }
         w.dev_prims_count = 0;
+        w.release_device = &release_prims;
         auto upload = [](void** dst, const void* src, size_t bytes) {
             if (bytes == 0) return cudaSuccess;
             cudaError_t r = cudaMalloc(dst, bytes);

@@ -56,6 +56,9 @@ struct Workload {
     void* dev_nodes = nullptr;
     void* dev_tris = nullptr;
     int dev_prims_device = -1;
+    // Frees the device tables above; set by the CUDA producers when they
+    // upload them (the host-only library never does).
+    void (*release_device)(Workload&) = nullptr;
     uint32_t dev_prims_count = 0;
 
     bool build();

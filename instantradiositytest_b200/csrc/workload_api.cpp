@@ -180,6 +180,12 @@ irt_status irt_workload_preset(int32_t which, irt_workload_spec* s) {
     return IRT_E_INVALID;
 }
 
+void irt_workload_destroy(irt_workload* wl) {
+    if (!wl) return;
+    if (wl->w.release_device) wl->w.release_device(wl->w);
+    delete wl;
+}
+
 irt_status irt_workload_create(const irt_workload_spec* spec, irt_workload** out) {
     if (!spec || !out) return IRT_E_INVALID;
     if (spec->width == 0 || spec->height == 0 || spec->width > 8192 || spec->height > 8192) return IRT_E_INVALID;

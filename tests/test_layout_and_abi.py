@@ -99,3 +99,25 @@ def test_checked_build_exports_the_same_abi():
     checked.irt_build_flavour.restype = C.c_char_p
     assert checked.irt_build_flavour() == b"checked"
     assert L.lib.irt_build_flavour() == (b"checked" if L.LIB_PATH == L.CHECKED_LIB_PATH else b"default")
+
+
+def test_reference_arm_loads_no_cuda_code():
+    """bench.py's reference arm times the oracle; its inputs come from the
+    host-only library (libirt_host.so: generator, CPU producers, loader), so
+    the process maps neither libirt.so nor the CUDA runtime."""
+    import json
+    import subprocess
+    import sys
+
+    assert os.path.exists(L.HOST_LIB_PATH), "build it with make -C instantradiositytest_b200"
+    code = ("import sys, runpy\n"
+            "sys.argv = ['bench.py', '--impl', 'reference', '--config', '0', '--steps', '1', '--warmup', '1',"
+            " '--reference-seconds', '1']\n"
+            "runpy.run_path('bench.py', run_name='__main__')\n"
+            "maps = open('/proc/self/maps').read()\n"
+            "print('MAPS', 'libirt.so' in maps, 'libirt_host.so' in maps, 'libcudart' in maps)\n")
+    r = subprocess.run([sys.executable, "-c", code], cwd=ROOT, capture_output=True, text=True, timeout=300)
+    assert r.returncode == 0, r.stderr[-2000:]
+    line = json.loads([x for x in r.stdout.splitlines() if x.startswith("{")][-1])
+    assert line["impl"] == "reference" and line["value"] > 0
+    assert r.stdout.strip().splitlines()[-1] == "MAPS False True False"
