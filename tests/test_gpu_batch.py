@@ -110,6 +110,35 @@ def test_batch_in_waves_equals_alone(cuda):
     ctx.close()
 
 
+def test_batch_large_views_equal_alone(cuda):
+    """Views whose ray queues are long enough that the march's warps reserve
+    queue entries in chunks (800x500: 800 000 rays, more than two chunks per
+    warp of the grid), beside a short one that takes entries one by one:
+    every ray is marched exactly once, so each view equals its render alone."""
+    a = workload(41, 16, 800, 500)
+    b = workload(42, 24, 800, 500)
+    c = workload(43, 8, 96, 64)
+    views = [(a, 0), (c, 0), (b, 0)]
+    ctx = Context()
+    drv = BatchDriver(ctx, views, use_graphs=False)
+    per_view = [[] for _ in views]
+    for i in range(4):
+        data = drv.inputs(i)
+        frames = drv.step(i, data)
+        for v, (f, (_, obj, nodes, lights)) in enumerate(zip(frames, data)):
+            per_view[v].append((L.Frame.from_buffer_copy(f), obj, nodes, lights))
+    torch.cuda.synchronize()
+    for v, (wl, _) in enumerate(views):
+        s = drv.batch.view(v)
+        ref = render_alone(ctx, wl, per_view[v], L.GBUFFER_F32, L.RADIANCE_F32, L.MOMENTS_F32)
+        for w in BUFS:
+            assert np.array_equal(s.buffer(w, torch.uint8).cpu().numpy(), ref[w]), (v, w)
+        for d in (0, 1):
+            assert np.array_equal(s.reservoirs_host(d, 2).view(np.uint8), ref["res"][d]), (v, d)
+    drv.close()
+    ctx.close()
+
+
 class _ViewShim:
     """What sync_history reads of a driver: the view's session and format."""
 
