@@ -292,8 +292,10 @@ irt_status irt_render_frame(irt_session* s, const irt_scene* scene, const irt_fr
  * slots, three VPL pools, created on the first call) on the session's own
  * copy stream while the previous frame still renders on `stream`; the frame
  * renders on `stream` once its inputs have landed, and, with out_host, its
- * filtered image (radiance format) is copied back to out_host on the copy
- * stream.  Call irt_session_host_sync before reading out_host.  The
+ * filtered image (radiance format) is copied back to out_host on a second
+ * copy stream — queued by the next call to run after that call's march, or
+ * by irt_session_host_sync.  Call irt_session_host_sync before reading
+ * out_host.  The
  * previous VPL pool of a call is the pool of the session's previous call
  * (zeros on the first).  No counterpart in the reference (its inputs are
  * GPU render targets). */

@@ -852,6 +852,22 @@ static irt_status pipe_setup(irt_session* s) {
     return IRT_OK;
 }
 
+// Queues the host copy of the last call's image (after the latest march
+// when `after_march`).
+static irt_status flush_output(irt_session* s, bool after_march) {
+    irt_context* ctx = s->ctx;
+    irt_session::HostPipe& hp = s->pipe;
+    if (!hp.pending_out) return IRT_OK;
+    const int slot = hp.pending_slot;
+    CK(cudaStreamWaitEvent(hp.copy_out, hp.out_ready[slot], 0), "pipeline wait");
+    if (after_march) CK(cudaStreamWaitEvent(hp.copy_out, hp.march_done, 0), "pipeline wait");
+    CK(cudaMemcpyAsync(hp.pending_out, hp.out[slot], s->P * s->rad_bytes, cudaMemcpyDeviceToHost, hp.copy_out),
+       "output");
+    CK(cudaEventRecord(hp.out_done[slot], hp.copy_out), "pipeline event");
+    hp.pending_out = nullptr;
+    return IRT_OK;
+}
+
 irt_status irt_render_frame_host(irt_session* s, const irt_scene* sc, const irt_frame* f, const irt_gbuffer* host_g,
                                  const irt_vpl* host_vpls, void* out_host, void* stream) {
     if (!s || !sc || !f || !host_g || !host_vpls) return IRT_E_INVALID;
@@ -905,15 +921,19 @@ irt_status irt_render_frame_host(irt_session* s, const irt_scene* sc, const irt_
     // The pool this frame read as `previous` is free after it; the current
     // one is the next frame's previous.
     if (hp.last_vpl >= 0) CK(cudaEventRecord(hp.vpl_free[hp.last_vpl], st), "pipeline event");
+    // The previous call's image goes to the host after this frame's march,
+    // beside this frame's SVGF passes (and the next inputs), like the uploads:
+    // during the march the copy's traffic through L2 slows it.
+    irt_status fr = flush_output(s, true);
+    if (fr) return fr;
     if (out_host) {
-        // A device copy of the output (the next frame overwrites the image),
-        // then the host copy on the copy stream.
+        // A device copy of the output (the next frame overwrites the image);
+        // its host copy is queued by the next call or irt_session_host_sync.
         CK(cudaStreamWaitEvent(st, hp.out_done[slot], 0), "pipeline wait");
         CK(cudaMemcpyAsync(hp.out[slot], s->filtered, P * s->rad_bytes, cudaMemcpyDeviceToDevice, st), "output");
         CK(cudaEventRecord(hp.out_ready[slot], st), "pipeline event");
-        CK(cudaStreamWaitEvent(hp.copy_out, hp.out_ready[slot], 0), "pipeline wait");
-        CK(cudaMemcpyAsync(out_host, hp.out[slot], P * s->rad_bytes, cudaMemcpyDeviceToHost, hp.copy_out), "output");
-        CK(cudaEventRecord(hp.out_done[slot], hp.copy_out), "pipeline event");
+        hp.pending_out = out_host;
+        hp.pending_slot = slot;
     }
     hp.last_vpl = vslot;
     hp.calls++;
@@ -925,6 +945,8 @@ irt_status irt_session_host_sync(irt_session* s, void* stream) {
     irt_context* ctx = s->ctx;
     if (!s->pipe.ready) return IRT_OK;
     DeviceGuard dg(ctx->device);
+    irt_status fr = flush_output(s, false);
+    if (fr) return fr;
     if (!stream) {
         CK(cudaStreamSynchronize(s->pipe.copy), "host inputs");
         CK(cudaStreamSynchronize(s->pipe.copy_out), "host outputs");

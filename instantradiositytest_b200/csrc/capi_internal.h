@@ -131,6 +131,8 @@ struct irt_session {
         void* out[2] = {nullptr, nullptr};
         cudaEvent_t copied[2] = {}, rendered[2] = {}, vpl_free[3] = {}, out_ready[2] = {}, out_done[2] = {};
         cudaEvent_t march_done = nullptr;  // after the last frame's march (recorded by irt_frame_lighting)
+        void* pending_out = nullptr;        // host destination of the last call's image, copied at the next call
+        int pending_slot = 0;               // ... from out[pending_slot]
         uint32_t calls = 0;
         int last_vpl = -1;
         uint64_t bytes = 0;
