@@ -542,9 +542,14 @@ irt_status irt_session_create(irt_context* ctx, const irt_session_desc* desc, ir
     return IRT_OK;
 }
 
+static irt_status flush_output(irt_session* s, bool after_march);
+
 void irt_session_destroy(irt_session* s) {
     if (!s) return;
     DeviceGuard g(s->ctx->device);
+    // The last call's image still goes to its host buffer, as it would at
+    // irt_session_host_sync.
+    if (s->pipe.ready) flush_output(s, false);
     void* ptrs[] = {s->dres[0], s->dres[1], s->dres[2], s->ires[0], s->ires[1], s->ires[2], s->archive,
                     s->prev_depth, s->prev_normal, s->direct, s->noisy, s->moments[0], s->moments[1],
                     s->feedback[0], s->feedback[1], s->temporal, s->scratch[0], s->scratch[1], s->filtered, s->error,

@@ -20,11 +20,14 @@ def test_host_inputs_equal_device_inputs(cuda, gfmt):
     scene = Scene(ctx, wl.meshes, wl.atlas, wl.sdf_format)
     sess = Session(ctx, session_desc(wl.settings, gfmt))
     outs = []
+    wants = []
     keep = []
-    for i in range(7):
+
+    def frame(i):
         inputs = ref.inputs(i)
         f, obj, nodes, lights, planes, vpls = inputs
         ref.step(i, inputs=inputs)
+        wants.append(ref.session.buffer(L.BUF_FILTERED, torch.uint8).cpu().numpy())
         g = {k: torch.from_numpy(np.ascontiguousarray(v).view(np.uint8).reshape(-1)).pin_memory()
              for k, v in planes.items()}
         hg = L.GBuffer(gfmt, g["depth"].data_ptr(), g["normal"].data_ptr(), g["color"].data_ptr(),
@@ -35,15 +38,25 @@ def test_host_inputs_equal_device_inputs(cuda, gfmt):
         sess.render_host(scene, f, hg, hv, out)
         keep.append((g, hv))  # host inputs must outlive their copies
         outs.append(out)
+
+    for i in range(7):
+        frame(i)
     sess.host_sync()
     torch.cuda.synchronize()
-    want = ref.session.buffer(L.BUF_FILTERED, torch.uint8).cpu().numpy()
-    assert np.array_equal(outs[-1].numpy(), want)
+    want = wants[-1]
+    # Every call's image reaches its host buffer (each is copied after the
+    # next call's march, the last at irt_session_host_sync).
+    for i in range(7):
+        assert np.array_equal(outs[i].numpy(), wants[i]), i
     assert np.array_equal(sess.buffer(L.BUF_FILTERED, torch.uint8).cpu().numpy(), want)
     for d in (0, 1):
         assert np.array_equal(sess.reservoirs_host(d, 2).view(np.uint8), ref.session.reservoirs_host(d, 2).view(np.uint8))
     assert np.abs(outs[-1].numpy().view(np.float32)).max() > 0
+    # One more call, then the session closed without irt_session_host_sync:
+    # its image still arrives.
+    frame(7)
     sess.close()
+    assert np.array_equal(outs[7].numpy(), wants[7])
     scene.close()
     ref.close()
     ctx.close()
