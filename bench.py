@@ -113,6 +113,9 @@ def parse():
     ap.add_argument("--reference-seconds", type=float, default=150.0, help="CPU budget of the reference arm")
     ap.add_argument("--serve-seconds", type=float, default=6.0, help="arrival window of the serving workload")
     ap.add_argument("--serve-streams", type=int, default=2)
+    ap.add_argument("--serve-rate", type=float, default=4.0,
+                    help="config 4: Poisson arrival rate of sessions per second (the workload's 4/s by default; "
+                         "a lower rate measures latency at a load the device sustains)")
     ap.add_argument("--no-paced-plain", action="store_true",
                     help="config 4: skip the arm that serves the requests one at a time at 60 fps")
     ap.add_argument("--field-filter", type=int, default=0, choices=[0, 1],
@@ -813,6 +816,7 @@ def serve(args):
     if rank != 0 and world > 1:
         return
     reqs, served, plain, t_build, scene_bytes, paced = serve_measure(args.serve_seconds, args.serve_streams,
+                                                                     rate=args.serve_rate,
                                                                      paced_plain=not args.no_paced_plain)
     gfmt, rfmt, mfmt, storage = storage_of(2)
     frames = int(served["frames"])
@@ -821,7 +825,7 @@ def serve(args):
         "steps": frames, "warmup": 0, "ms_per_step": 1000.0 * served["seconds"] / max(frames, 1),
         "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f32", "data": "synthetic",
         "impl": "ours",
-        "config": {"workload": f"serving: Poisson arrivals 4/s over {args.serve_seconds} s "
+        "config": {"workload": f"serving: Poisson arrivals {args.serve_rate:g}/s over {args.serve_seconds} s "
                                f"({len(reqs)} sessions), 8-64 meshes, resolutions {SERVE_RESOLUTIONS}, "
                                f"U(30,300) frames at 60 fps, 160 GB admission budget",
                    "storage": storage, "streams": args.serve_streams,
