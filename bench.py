@@ -597,7 +597,8 @@ def ours(args):
     march_flops = None
     if counters:
         march_flops = sum(FLOPS_PER[k] * counters.get(k, 0.0) for k in FLOPS_PER)
-    traffic = ncu_traffic(dominant, f"{W}x{H}" + ("_mixed" if args.config == 2 else ""))
+    suffix = "_mixed" if args.config == 2 else ("_field_linear" if args.field_filter else "")
+    traffic = ncu_traffic(dominant, f"{W}x{H}{suffix}")
     kernels = {n: {"ms": float(mean_ms[kernel_idx[n]]), "alg_GBps": ach(n), "frac": ach(n) / peak} for n in KERNELS}
     hbm = {"achieved": ach(dominant), "peak": peak, "unit": "GB/s", "frac": ach(dominant) / peak,
            "peak_source": peak_kind, "alg_bytes_per_pixel": alg[dominant]}
