@@ -24,9 +24,11 @@ def workload(seed, meshes, w, h):
                                 n_spheres=(meshes - 1) - (meshes - 1) * 6 // 10))
 
 
-def render_alone(ctx, wl, frames, fmt, rfmt, mfmt):
+def render_alone(ctx, wl, frames, fmt, rfmt, mfmt, field_filter=None):
     """One session over `frames` (the batch's frames of the view)."""
     scene = Scene(ctx, wl.meshes, wl.atlas, wl.sdf_format)
+    if field_filter is not None:
+        scene.set_field_filter(field_filter)
     sess = Session(ctx, session_desc(wl.settings, fmt, rfmt, 1, False, False, mfmt))
     _, gs = gbuffer_device_alloc(wl.height, wl.width, fmt)
     pools = [torch.zeros(wl.settings.vpl_count * 48, dtype=torch.uint8, device="cuda") for _ in range(3)]
@@ -135,6 +137,37 @@ def test_batch_large_views_equal_alone(cuda):
             assert np.array_equal(s.buffer(w, torch.uint8).cpu().numpy(), ref[w]), (v, w)
         for d in (0, 1):
             assert np.array_equal(s.reservoirs_host(d, 2).view(np.uint8), ref["res"][d]), (v, d)
+    drv.close()
+    ctx.close()
+
+
+def test_batch_linear_field_views_equal_alone(cuda):
+    """Views of scenes whose field sampler is the hardware-filtered one (f32
+    atlases): the batched march takes the sampler from each scene group's
+    record, so every view equals its render alone with that sampler, and
+    differs from the point-sampled render."""
+    a = Workload(preset_spec(1, seed=51, width=160, height=100, n_boxes=6, n_spheres=5))
+    b = Workload(preset_spec(1, seed=52, width=224, height=140, n_boxes=8, n_spheres=7))
+    views = [(a, 0), (b, 0), (a, 5)]
+    ctx = Context()
+    drv = BatchDriver(ctx, views, use_graphs=True)
+    for scene in drv.scenes.values():
+        scene.set_field_filter(L.FIELD_LINEAR)
+    per_view = [[] for _ in views]
+    for i in range(6):
+        data = drv.inputs(i)
+        frames = drv.step(i, data)
+        for v, (f, (_, obj, nodes, lights)) in enumerate(zip(frames, data)):
+            per_view[v].append((L.Frame.from_buffer_copy(f), obj, nodes, lights))
+    torch.cuda.synchronize()
+    for v, (wl, _) in enumerate(views):
+        s = drv.batch.view(v)
+        ref = render_alone(ctx, wl, per_view[v], L.GBUFFER_F32, L.RADIANCE_F32, L.MOMENTS_F32, L.FIELD_LINEAR)
+        for w in BUFS:
+            assert np.array_equal(s.buffer(w, torch.uint8).cpu().numpy(), ref[w]), (v, w)
+    point = render_alone(ctx, a, per_view[0], L.GBUFFER_F32, L.RADIANCE_F32, L.MOMENTS_F32, L.FIELD_POINT)
+    assert not np.array_equal(drv.batch.view(0).buffer(L.BUF_DIRECT, torch.uint8).cpu().numpy(),
+                              point[L.BUF_DIRECT])
     drv.close()
     ctx.close()
 
