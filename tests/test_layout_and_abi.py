@@ -121,3 +121,19 @@ def test_reference_arm_loads_no_cuda_code():
     line = json.loads([x for x in r.stdout.splitlines() if x.startswith("{")][-1])
     assert line["impl"] == "reference" and line["value"] > 0
     assert r.stdout.strip().splitlines()[-1] == "MAPS False True False"
+
+
+def test_committed_profiles_hold_the_bench_figures():
+    """bench.py takes the march's DRAM bytes per launch (the line's
+    roofline traffic) for each storage and field sampler, and its executed
+    FP32 flops per pixel, from the committed ncu summaries under profiles/."""
+    import importlib.util
+
+    spec = importlib.util.spec_from_file_location("bench_figures", os.path.join(ROOT, "bench.py"))
+    bench = importlib.util.module_from_spec(spec)
+    spec.loader.exec_module(bench)
+    for workload in ("1920x1200", "1920x1200_mixed", "1920x1200_field_linear"):
+        traffic = bench.ncu_traffic("march", workload)
+        assert traffic is not None and 3.13e8 <= traffic < 2e9, (workload, traffic)
+    flops = bench.ncu_figure("march", "1920x1200", "executed_fp32_flops_per_pixel")
+    assert flops is not None and 1000 < flops < 20190
