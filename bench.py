@@ -699,7 +699,7 @@ def headline_runs(ctx, dev, schedule, plain_value, plain_frame_ms, args):
                                  f"{SERVE_RESOLUTIONS}, U(30,300) frames paced at 60 fps, mixed-precision storage, "
                                  f"160 GB admission budget, {args.serve_streams} streams; plain arm: the same "
                                  f"requests one at a time, unpaced")
-    out["target"] = ("north star: the served/batched FP16-storage form at >= 3x the plain single-view path's "
+    out["target"] = ("performance target: the served/batched FP16-storage form at >= 3x the plain single-view path's "
                      "Mpix-frames/s. served.over_plain_arm compares with the same requests rendered one session "
                      "at a time as fast as the device allows (its throughput); served.over_plain_paced with "
                      "one session at a time at the sessions' 60 fps (a queue without continuous batching)")
@@ -806,7 +806,7 @@ def paced_plain_estimate(reqs, plain):
 
 
 def serve(args):
-    """Serving workload as its own JSON line: sessions
+    """The serving workload (render sessions arriving over a window) as its own JSON line: sessions
     arriving at 4/s, admitted against a 160 GB budget, frames paced at
     60 fps, mixed-precision storage, against the same requests run session
     by session."""
