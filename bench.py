@@ -114,10 +114,10 @@ def parse():
     ap.add_argument("--serve-seconds", type=float, default=6.0, help="arrival window of the serving workload")
     ap.add_argument("--serve-streams", type=int, default=2)
     ap.add_argument("--serve-rate", type=float, default=4.0,
-                    help="config 4: Poisson arrival rate of sessions per second (the workload's 4/s by default; "
+                    help="with --config 4: Poisson arrival rate of sessions per second (the workload's 4/s by default; "
                          "a lower rate measures latency at a load the device sustains)")
     ap.add_argument("--no-paced-plain", action="store_true",
-                    help="config 4: skip the arm that serves the requests one at a time at 60 fps")
+                    help="with --config 4: skip the arm that serves the requests one at a time at 60 fps")
     ap.add_argument("--field-filter", type=int, default=0, choices=[0, 1],
                     help="SDF sampler: 0 point-sampled trilinear (default), 1 the reference's hardware-filtered one")
     ap.add_argument("--no-headline", action="store_true",
