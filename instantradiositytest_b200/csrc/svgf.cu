@@ -120,11 +120,14 @@ __device__ __forceinline__ void temporal_body(const irt_frame& f, const SvgfCtx<
     M::store(moments_out, i, Moments{m0, M::central ? sqrtf(variance) : m1, age});
 }
 
-// At most 64 registers (4 blocks of 256 per SM): the f16-moments forms
-// would take 80 (3 blocks), and with their small spills the mixed-precision
-// pass runs 0.394 -> 0.334 ms per 1920x1200 frame; the f32 form is unchanged.
+// Held to 32 registers (8 blocks of 256, every warp slot of the SM): the pass
+// waits on its history and neighbour gathers, and more resident warps hide
+// more of that than the spills cost.  Per 1920x1200 frame, f32 / mixed
+// storage: 3 blocks by registers (the f16-moments forms take 80) 0.302 /
+// 0.394 ms, 4 blocks 0.299 / 0.334, 5 blocks 0.266 / 0.308, 6 blocks 0.266 /
+// 0.290, 8 blocks 0.254 / 0.296 ms.
 template <class G, class R, class M>
-__global__ void __launch_bounds__(256, 4) svgf_temporal_kernel(const __grid_constant__ irt_frame f, const __grid_constant__ SvgfCtx<G> c,
+__global__ void __launch_bounds__(256, 8) svgf_temporal_kernel(const __grid_constant__ irt_frame f, const __grid_constant__ SvgfCtx<G> c,
                                                             const typename R::T* noisy, const typename R::T* old_radiance,
                                                             const typename M::T* old_moments, typename R::T* radiance_out,
                                                             typename M::T* moments_out) {
@@ -133,7 +136,7 @@ __global__ void __launch_bounds__(256, 4) svgf_temporal_kernel(const __grid_cons
 }
 
 template <class G, class R, class M>
-__global__ void __launch_bounds__(256, 4) svgf_temporal_batched(const irt_frame* __restrict__ frames,
+__global__ void __launch_bounds__(256, 8) svgf_temporal_batched(const irt_frame* __restrict__ frames,
                                                              const SView<G>* __restrict__ views,
                                                              const uint32_t* __restrict__ tile_start, uint32_t n) {
     const uint32_t v = svgf_find_view(tile_start, n, blockIdx.x);
