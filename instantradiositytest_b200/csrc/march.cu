@@ -45,10 +45,14 @@ namespace exact {
 #endif
 
 enum : uint32_t { kClear = 0, kEndpoint = 1, kMarch = 2 };
-// CTAs of 128 threads resident per SM: 64 registers a thread, no spills
-// (9 CTAs at 56 registers spill and measured 3.82 ms; 7 CTAs 3.78 ms; 8 CTAs 3.56 ms
-// per 1920x1200 frame).
+// Resident warps: 64 registers a thread, no spills, 32 warps per SM.  In
+// CTAs of 128 threads (the batched march): 9 CTAs at 56 registers spill and
+// measured 3.82 ms, 7 CTAs 3.78 ms, 8 CTAs 3.56 ms per 1920x1200 frame.  The
+// single-view march runs them as 4 CTAs of 256 threads, each staging the
+// scene records once for 8 warps: 3.392 -> 3.371 ms against 8 CTAs of 128.
 constexpr int kMarchBlocksPerSm = 8;
+constexpr int kMarchThreads = 256;
+constexpr int kMarchCtasPerSm = 4;
 // Queue entries a warp reserves per atomic (one per lane): the queue counter
 // then sees one atomic per ~30 warp iterations instead of about one per
 // iteration (1920x1200 room: 3.51 -> 3.43 ms with the L2 prefetch of the
@@ -262,7 +266,7 @@ __device__ __forceinline__ void march_reset(MarchState& m) {
     m.step = 0;
 }
 
-__global__ void __launch_bounds__(128, kMarchBlocksPerSm) march_kernel(const __grid_constant__ irt_frame f, const DevScene sc,
+__global__ void __launch_bounds__(kMarchThreads, kMarchCtasPerSm) march_kernel(const __grid_constant__ irt_frame f, const DevScene sc,
                                                     const float4* __restrict__ march_scene, uint32_t scene_vec4,
                                                     const Grid grid, const RayRecord* __restrict__ rays,
                                                     uint32_t* counters, float* __restrict__ vis) {
@@ -484,9 +488,9 @@ cudaError_t IRT_MARCH_LAUNCH(const MarchLaunch& M, cudaStream_t st) {
         configured_device = device;
         cudaError_t e = cudaFuncSetAttribute(march_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
         if (e != cudaSuccess) return e;
-        e = march_prefer_l1((const void*)march_kernel, smem, kMarchBlocksPerSm);
+        e = march_prefer_l1((const void*)march_kernel, smem, kMarchCtasPerSm);
         if (e != cudaSuccess) return e;
-        e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&blocks_per_sm, march_kernel, 128, smem);
+        e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&blocks_per_sm, march_kernel, kMarchThreads, smem);
         if (e != cudaSuccess) return e;
         if (blocks_per_sm < 1) return cudaErrorInvalidConfiguration;
         configured_smem = smem;
@@ -509,7 +513,7 @@ cudaError_t IRT_MARCH_LAUNCH(const MarchLaunch& M, cudaStream_t st) {
     g.ix = M.grid_inv[0];
     g.iy = M.grid_inv[1];
     g.iz = M.grid_inv[2];
-    march_kernel<<<M.num_sms * blocks_per_sm, 128, smem, st>>>(*M.frame, sc, M.march_scene, smem / 16, g, M.rays,
+    march_kernel<<<M.num_sms * blocks_per_sm, kMarchThreads, smem, st>>>(*M.frame, sc, M.march_scene, smem / 16, g, M.rays,
                                                                 M.ray_counters, M.vis);
     return cudaGetLastError();
 }
